@@ -1,0 +1,157 @@
+"""ctypes bindings for the reference library shim (oracle/_ref/libtfhe_ref_shim.so).
+
+Test infrastructure: drives the unmodified reference (tfhe v1.1, spqlios-fma) built from its own
+sources by oracle/ref.mk.  Used to generate golden vectors, to run the reference live on identical
+inputs when its build is present, and as the timed CPU baseline.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+SHIM = os.path.join(REF_DIR, "libtfhe_ref_shim.so")
+
+_V = ctypes.c_void_p
+_I = ctypes.c_int32
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_V)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class RefKeys:
+    """A reference TFheGateBootstrappingSecretKeySet plus raw accessors."""
+
+    def __init__(self, lib, handle):
+        self.lib = lib
+        self.h = _V(handle)
+        d = np.zeros(8, np.int32)
+        lib.rs_dims(self.h, _p(d))
+        self.n, self.N, self.k, self.l, self.Bgbit, self.ks_t, self.ks_basebit, self.kpl = map(int, d)
+
+    def params(self):
+        return dict(n=self.n, N=self.N, k=self.k, l=self.l, Bgbit=self.Bgbit,
+                    ks_t=self.ks_t, ks_basebit=self.ks_basebit)
+
+    def export(self, bsk=True, ksk=True):
+        n, N, k = self.n, self.N, self.k
+        lk = np.zeros(n, np.int32)
+        tk = np.zeros(k * N, np.int32)
+        kk = np.zeros((k * N, self.ks_t, 1 << self.ks_basebit, n + 1), np.int32) if ksk else None
+        bk = np.zeros((n, self.kpl, k + 1, N), np.int32) if bsk else None
+        self.lib.rs_export(self.h, _p(lk), _p(tk), _p(kk), _p(bk))
+        return lk, tk, kk, bk
+
+    def encrypt(self, bits):
+        bits = _i32(bits)
+        out = np.zeros((len(bits), self.n + 1), np.int32)
+        self.lib.rs_encrypt(self.h, len(bits), _p(bits), _p(out))
+        return out
+
+    def decrypt(self, cts):
+        cts = _i32(cts)
+        bits = np.zeros(len(cts), np.int32)
+        ph = np.zeros(len(cts), np.int32)
+        self.lib.rs_decrypt(self.h, len(cts), _p(cts), _p(bits), _p(ph))
+        return bits, ph
+
+    def gate(self, code, a, b=None, c=None):
+        a = _i32(a)
+        b = None if b is None else _i32(b)
+        c = None if c is None else _i32(c)
+        out = np.zeros_like(a)
+        self.lib.rs_gate(self.h, code, len(a), _p(a), _p(b), _p(c), _p(out))
+        return out
+
+    def bootstrap_woks(self, mu, x):
+        x = _i32(x)
+        out = np.zeros((len(x), self.k * self.N + 1), np.int32)
+        self.lib.rs_bootstrap_woks(self.h, mu, len(x), _p(x), _p(out))
+        return out
+
+    def keyswitch(self, x):
+        x = _i32(x)
+        out = np.zeros((len(x), self.n + 1), np.int32)
+        self.lib.rs_keyswitch(self.h, len(x), _p(x), _p(out))
+        return out
+
+    def extern_mul(self, i, acc):
+        acc = _i32(acc).copy()
+        self.lib.rs_extern_mul(self.h, i, _p(acc))
+        return acc
+
+    def bench_gates(self, code, threads, per_thread, a, b, c, out):
+        return self.lib.rs_bench_gates(self.h, code, threads, per_thread, _p(a), _p(b), _p(c), _p(out))
+
+    def free(self):
+        if self.h is not None:
+            self.lib.rs_free(self.h)
+            self.h = None
+
+
+class RefLib:
+    _inst = None
+
+    def __init__(self, path):
+        L = ctypes.CDLL(path)
+        L.rs_keygen.restype = _V
+        L.rs_keygen.argtypes = [ctypes.c_int] * 8 + [ctypes.c_double] * 2 + [ctypes.c_uint32]
+        L.rs_bench_gates.restype = ctypes.c_double
+        L.rs_bench_gates.argtypes = [_V, ctypes.c_int, _I, _I, _V, _V, _V, _V]
+        L.rs_dtot32.argtypes = [ctypes.c_double]
+        self.L = L
+
+    @classmethod
+    def available(cls):
+        return os.path.exists(SHIM)
+
+    @classmethod
+    def load(cls, required=False):
+        if cls._inst is None:
+            if not os.path.exists(SHIM):
+                if required:
+                    raise RuntimeError(f"reference build missing: {SHIM} (run make -f oracle/ref.mk)")
+                return None
+            cls._inst = RefLib(SHIM)
+        return cls._inst
+
+    def keygen(self, custom=None, ks_stdev=2**-15, bk_stdev=2**-25, seed=1):
+        if custom is None:
+            h = self.L.rs_keygen(0, 0, 0, 0, 0, 0, 0, 0, 0.0, 0.0, seed)
+        else:
+            p = custom
+            h = self.L.rs_keygen(1, p["n"], p["N"], p["k"], p["l"], p["Bgbit"], p["ks_t"], p["ks_basebit"],
+                                 ks_stdev, bk_stdev, seed)
+        return RefKeys(self.L, h)
+
+    def modswitch_from(self, phase, msize):
+        return self.L.rs_modswitch_from(phase, msize)
+
+    def modswitch_to(self, mu, msize):
+        return self.L.rs_modswitch_to(mu, msize)
+
+    def decompose(self, N, l, bgbit, poly):
+        out = np.zeros((l, N), np.int32)
+        self.L.rs_decompose(N, l, bgbit, _p(_i32(poly)), _p(out))
+        return out
+
+    def rotate(self, N, a, minus_one, poly):
+        out = np.zeros(N, np.int32)
+        self.L.rs_rotate(N, a, 1 if minus_one else 0, _p(_i32(poly)), _p(out))
+        return out
+
+    def extract(self, N, k, tlwe):
+        out = np.zeros(k * N + 1, np.int32)
+        self.L.rs_extract(N, k, _p(_i32(tlwe)), _p(out))
+        return out
+
+    def poly_mult(self, kind, N, ipoly, tpoly):
+        out = np.zeros(N, np.int32)
+        self.L.rs_poly_mult(kind, N, _p(_i32(ipoly)), _p(_i32(tpoly)), _p(out))
+        return out
