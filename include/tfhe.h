@@ -1,0 +1,159 @@
+/*
+ * tfhe.h -- drop-in replacement for the gate-bootstrapping API of tfhe v1.1, served by
+ * libtfhe_b200.so.  A program written against the reference's tfhe.h gate API
+ * (tfhe_gate_bootstrapping_functions.h:14-89) compiles against this header unchanged and links
+ * with -ltfhe_b200 instead of -ltfhe-spqlios-fma.
+ *
+ * Struct layouts visible to callers keep the reference's field order and types:
+ *   LweParams        lweparams.h:13-16          LweSample   lwesamples.h:9-12
+ *   TLweParams       tlwe.h:10-15               LweKey      lwekey.h:10-12
+ *   TGswParams       tgsw.h:10-19
+ *   TFheGateBootstrappingParameterSet / CloudKeySet / SecretKeySet
+ *                    tfhe_gate_bootstrapping_structures.h:9-63
+ * TGswKey, LweBootstrappingKey and LweBootstrappingKeyFFT are opaque here; the cloud keyset's
+ * bkFFT points at the engine's device-resident key.
+ *
+ * Every bootstrapped gate runs on the GPU (no CPU fallback).  The drop-in keeps the reference's
+ * FP64 precision by default; tfhe_b200_set_precision selects the split-FP32 form.
+ */
+#ifndef TFHE_B200_DROPIN_TFHE_H
+#define TFHE_B200_DROPIN_TFHE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+#define TFHE_B200_EXPORT extern "C"
+#else
+#define TFHE_B200_EXPORT
+#endif
+
+typedef int32_t Torus32;
+
+typedef struct LweParams {
+    const int32_t n;
+    const double alpha_min;
+    const double alpha_max;
+} LweParams;
+
+typedef struct TLweParams {
+    const int32_t N;
+    const int32_t k;
+    const double alpha_min;
+    const double alpha_max;
+    const LweParams extracted_lweparams;
+} TLweParams;
+
+typedef struct TGswParams {
+    const int32_t l;
+    const int32_t Bgbit;
+    const int32_t Bg;
+    const int32_t halfBg;
+    const uint32_t maskMod;
+    const TLweParams *tlwe_params;
+    const int32_t kpl;
+    Torus32 *h;
+    uint32_t offset;
+} TGswParams;
+
+typedef struct LweSample {
+    Torus32 *a;
+    Torus32 b;
+    double current_variance;
+} LweSample;
+
+typedef struct LweKey {
+    const LweParams *params;
+    int32_t *key;
+} LweKey;
+
+typedef struct TGswKey TGswKey;
+typedef struct LweBootstrappingKey LweBootstrappingKey;
+typedef struct LweBootstrappingKeyFFT LweBootstrappingKeyFFT;
+
+typedef struct TFheGateBootstrappingParameterSet {
+    const int32_t ks_t;
+    const int32_t ks_basebit;
+    const LweParams *const in_out_params;
+    const TGswParams *const tgsw_params;
+} TFheGateBootstrappingParameterSet;
+
+typedef struct TFheGateBootstrappingCloudKeySet {
+    const TFheGateBootstrappingParameterSet *const params;
+    const LweBootstrappingKey *const bk;
+    const LweBootstrappingKeyFFT *const bkFFT;
+} TFheGateBootstrappingCloudKeySet;
+
+typedef struct TFheGateBootstrappingSecretKeySet {
+    const TFheGateBootstrappingParameterSet *params;
+    const LweKey *lwe_key;
+    const TGswKey *tgsw_key;
+    const TFheGateBootstrappingCloudKeySet cloud;
+} TFheGateBootstrappingSecretKeySet;
+
+/* ---- tfhe_gate_bootstrapping_functions.h:14-89 --------------------------------------------- */
+TFHE_B200_EXPORT TFheGateBootstrappingParameterSet *new_default_gate_bootstrapping_parameters(int32_t minimum_lambda);
+TFHE_B200_EXPORT TFheGateBootstrappingSecretKeySet *
+new_random_gate_bootstrapping_secret_keyset(const TFheGateBootstrappingParameterSet *params);
+TFHE_B200_EXPORT void delete_gate_bootstrapping_parameters(TFheGateBootstrappingParameterSet *params);
+TFHE_B200_EXPORT void delete_gate_bootstrapping_secret_keyset(TFheGateBootstrappingSecretKeySet *keyset);
+TFHE_B200_EXPORT void delete_gate_bootstrapping_cloud_keyset(TFheGateBootstrappingCloudKeySet *keyset);
+TFHE_B200_EXPORT LweSample *new_gate_bootstrapping_ciphertext(const TFheGateBootstrappingParameterSet *params);
+TFHE_B200_EXPORT LweSample *new_gate_bootstrapping_ciphertext_array(int32_t nbelems,
+                                                                    const TFheGateBootstrappingParameterSet *params);
+TFHE_B200_EXPORT void delete_gate_bootstrapping_ciphertext(LweSample *sample);
+TFHE_B200_EXPORT void delete_gate_bootstrapping_ciphertext_array(int32_t nbelems, LweSample *samples);
+TFHE_B200_EXPORT void bootsSymEncrypt(LweSample *result, int32_t message, const TFheGateBootstrappingSecretKeySet *params);
+TFHE_B200_EXPORT int32_t bootsSymDecrypt(const LweSample *sample, const TFheGateBootstrappingSecretKeySet *params);
+TFHE_B200_EXPORT void bootsCONSTANT(LweSample *result, int32_t value, const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsNAND(LweSample *result, const LweSample *ca, const LweSample *cb,
+                                const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsOR(LweSample *result, const LweSample *ca, const LweSample *cb,
+                              const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsAND(LweSample *result, const LweSample *ca, const LweSample *cb,
+                               const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsXOR(LweSample *result, const LweSample *ca, const LweSample *cb,
+                               const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsXNOR(LweSample *result, const LweSample *ca, const LweSample *cb,
+                                const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsNOT(LweSample *result, const LweSample *ca, const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsCOPY(LweSample *result, const LweSample *ca, const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsNOR(LweSample *result, const LweSample *ca, const LweSample *cb,
+                               const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsANDNY(LweSample *result, const LweSample *ca, const LweSample *cb,
+                                 const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsANDYN(LweSample *result, const LweSample *ca, const LweSample *cb,
+                                 const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsORNY(LweSample *result, const LweSample *ca, const LweSample *cb,
+                                const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsORYN(LweSample *result, const LweSample *ca, const LweSample *cb,
+                                const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsMUX(LweSample *result, const LweSample *a, const LweSample *b, const LweSample *c,
+                               const TFheGateBootstrappingCloudKeySet *bk);
+
+/* ---- tfhe.h:34 ------------------------------------------------------------------------------ */
+TFHE_B200_EXPORT void tfhe_random_generator_setSeed(uint32_t *values, int32_t size);
+
+/* ---- hot-path internals of tfhe.h:42-45 / lwe-functions.h:79, on the GPU -------------------- */
+TFHE_B200_EXPORT void tfhe_bootstrap_FFT(LweSample *result, const LweBootstrappingKeyFFT *bk, Torus32 mu,
+                                         const LweSample *x);
+TFHE_B200_EXPORT void tfhe_bootstrap_woKS_FFT(LweSample *result, const LweBootstrappingKeyFFT *bk, Torus32 mu,
+                                              const LweSample *x);
+TFHE_B200_EXPORT Torus32 modSwitchToTorus32(int32_t mu, int32_t Msize);
+TFHE_B200_EXPORT int32_t modSwitchFromTorus32(Torus32 phase, int32_t Msize);
+TFHE_B200_EXPORT Torus32 lwePhase(const LweSample *sample, const LweKey *key);
+
+/* ---- batched extensions (no reference counterpart: the reference evaluates one gate per call) -
+ * results[i] = gate(a[i], b[i] (, c[i])) for i < count, over arrays from
+ * new_gate_bootstrapping_ciphertext_array; one GPU launch sequence per call.
+ * gate codes as in tfhe_b200.h (0 NAND ... 10 MUX, 11 NOT, 12 COPY). */
+TFHE_B200_EXPORT void bootsGATE_batch(int32_t gate, LweSample *results, const LweSample *a, const LweSample *b,
+                                      const LweSample *c, int32_t count, const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsNAND_batch(LweSample *results, const LweSample *a, const LweSample *b, int32_t count,
+                                      const TFheGateBootstrappingCloudKeySet *bk);
+TFHE_B200_EXPORT void bootsMUX_batch(LweSample *results, const LweSample *a, const LweSample *b, const LweSample *c,
+                                     int32_t count, const TFheGateBootstrappingCloudKeySet *bk);
+
+/* 0 = FP64 (default), 1 = split FP32.  Applies to subsequent gate calls of this process. */
+TFHE_B200_EXPORT void tfhe_b200_set_precision(int32_t precision);
+
+#endif

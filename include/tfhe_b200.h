@@ -1,0 +1,156 @@
+/*
+ * tfhe_b200.h -- native C ABI of the B200 gate-bootstrapping engine (libtfhe_b200.so).
+ *
+ * Plain C: pointers, sizes and status codes only.  Ciphertexts are raw int32 arrays:
+ *   LWE ciphertext      [n+1]              a[0..n-1], b          (lwesamples.h:9-20: LweSample a, b)
+ *   batch of ciphertexts[count][n+1]       row-major
+ *   extracted sample    [k*N+1]            dimension of the extracted key (tlwe.h:15 extracted_lweparams)
+ * Gate codes follow boot-gates.cpp: 0 NAND 1 OR 2 AND 3 XOR 4 XNOR 5 NOR 6 ANDNY 7 ANDYN 8 ORNY
+ * 9 ORYN 10 MUX 11 NOT 12 COPY.
+ *
+ * Each entry point below names the reference interface it replaces (file:line in tfhe v1.1).
+ * The reference-compatible drop-in (same struct layouts and symbols as tfhe_gate_bootstrapping_
+ * functions.h) is declared in tfhe.h and implemented on top of this ABI.
+ */
+#ifndef TFHE_B200_H
+#define TFHE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    TFHEB_OK = 0,
+    TFHEB_ERR_INVALID = 1,     /* bad argument or size */
+    TFHEB_ERR_CUDA = 2,        /* CUDA runtime error (message in tfheb_last_error) */
+    TFHEB_ERR_NOMEM = 3,       /* device or host allocation failed */
+    TFHEB_ERR_UNSUPPORTED = 4, /* parameter set without a compiled kernel */
+    TFHEB_ERR_TIMEOUT = 5,     /* a bounded device-side wait expired */
+    TFHEB_ERR_NO_DEVICE = 6    /* no CUDA device visible */
+} tfheb_status;
+
+typedef enum {
+    TFHEB_FP64 = 0,       /* plain form: FP64 negacyclic FFT (the reference's precision) */
+    TFHEB_SPLIT_FP32 = 1  /* bootstrapping key split in two integer limbs, FP32 FFTs, exact recombination */
+} tfheb_precision;
+
+enum {
+    TFHEB_NAND = 0, TFHEB_OR = 1, TFHEB_AND = 2, TFHEB_XOR = 3, TFHEB_XNOR = 4, TFHEB_NOR = 5,
+    TFHEB_ANDNY = 6, TFHEB_ANDYN = 7, TFHEB_ORNY = 8, TFHEB_ORYN = 9, TFHEB_MUX = 10, TFHEB_NOT = 11,
+    TFHEB_COPY = 12
+};
+
+/* Gate-bootstrapping parameter set (tfhe_gate_bootstrapping_structures.h:9-24 with the LweParams,
+ * TLweParams and TGswParams it points to, flattened). */
+typedef struct {
+    int32_t n;          /* LWE dimension (lweparams.h:13-16) */
+    int32_t N;          /* ring degree (tlwe.h:10-15) */
+    int32_t k;          /* TLWE mask polynomials */
+    int32_t l;          /* gadget decomposition length (tgsw.h:10-19) */
+    int32_t Bgbit;      /* log2 of the gadget base */
+    int32_t ks_t;       /* keyswitch length */
+    int32_t ks_basebit; /* keyswitch log2 base */
+    double ks_stdev;    /* LWE / keyswitch noise stdev (alpha_min of the LWE params) */
+    double bk_stdev;    /* bootstrapping-key noise stdev (alpha_min of the TLWE params) */
+} tfheb_params;
+
+typedef struct tfheb_secret_key tfheb_secret_key;
+typedef struct tfheb_cloud_key tfheb_cloud_key;
+
+/* Last error message of the calling thread ("" if none). */
+const char *tfheb_last_error(void);
+
+/* Number of kernels this library launched on the calling process so far (all keys). */
+int64_t tfheb_kernel_launches(void);
+
+/* Replaces new_default_gate_bootstrapping_parameters (tfhe_gate_bootstrapping.cpp:77-89):
+ * lambda <= 80 -> the 80-bit set (:23-48), 80 < lambda <= 128 -> the 128-bit default (:51-75). */
+tfheb_status tfheb_default_params(int32_t lambda, tfheb_params *out);
+
+/* The larger-ring set n=800, N=2048, l=3, Bgbit=8 (no reference counterpart: the reference's FFT
+ * backends are fixed at N=1024, fft_processor_spqlios.cpp:123). */
+tfheb_status tfheb_large_params(tfheb_params *out);
+
+/* Replaces new_random_gate_bootstrapping_secret_keyset (tfhe_gate_bootstrapping.cpp:97-108):
+ * secret keys, keyswitching key and coefficient-domain bootstrapping key, from a seed. */
+tfheb_status tfheb_keygen(const tfheb_params *p, uint64_t seed, tfheb_secret_key **sk, tfheb_cloud_key **ck);
+
+/* Import keys generated elsewhere (e.g. by the reference library), raw layouts:
+ *   bsk [n][(k+1)*l][k+1][N] coefficient-domain TGSW rows (tgsw.h:55-60 all_sample order)
+ *   ksk [k*N][ks_t][2^ks_basebit][n+1] (lwekeyswitch.h:11-28 ks0_raw order)
+ *   lwe_key [n], tlwe_key [k][N]. */
+tfheb_status tfheb_cloud_key_import(const tfheb_params *p, const int32_t *bsk, const int32_t *ksk,
+                                    tfheb_cloud_key **ck);
+tfheb_status tfheb_secret_key_import(const tfheb_params *p, const int32_t *lwe_key, const int32_t *tlwe_key,
+                                     tfheb_secret_key **sk);
+tfheb_status tfheb_secret_key_export(const tfheb_secret_key *sk, int32_t *lwe_key, int32_t *tlwe_key);
+tfheb_status tfheb_cloud_key_export(const tfheb_cloud_key *ck, int32_t *bsk, int32_t *ksk);
+tfheb_status tfheb_cloud_key_params(const tfheb_cloud_key *ck, tfheb_params *out);
+/* Replaces delete_gate_bootstrapping_{secret,cloud}_keyset (tfhe_gate_bootstrapping.cpp:111-130). */
+void tfheb_secret_key_free(tfheb_secret_key *sk);
+void tfheb_cloud_key_free(tfheb_cloud_key *ck);
+
+/* Replaces bootsSymEncrypt / bootsSymDecrypt (tfhe_gate_bootstrapping.cpp:154-165):
+ * bits -> [count][n+1] with noise stdev ks_stdev; decrypt returns bits and optional raw phases. */
+tfheb_status tfheb_encrypt(const tfheb_secret_key *sk, const int32_t *bits, int32_t count, uint64_t seed,
+                           int32_t *out);
+tfheb_status tfheb_decrypt(const tfheb_secret_key *sk, const int32_t *cts, int32_t count, int32_t *bits,
+                           int32_t *phases);
+
+/* Moves the cloud key to a GPU: FFT-domain bootstrapping key in the requested precisions
+ * (bit 0 = FP64, bit 1 = split FP32), keyswitching key, twiddle tables.  The host-side FP64
+ * transform replaces init_LweBootstrappingKeyFFT (lwe-bootstrapping-functions-fft.cpp:23-52).
+ * split_shift: weight 2^split_shift of the high limb in split mode (0 = default 24). */
+tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *ck, int32_t device, int32_t precision_mask,
+                                       int32_t split_shift);
+
+/* Batched gates on host buffers ([count][n+1] each; c only for MUX, b unused for NOT/COPY):
+ * the batched counterpart of bootsNAND...bootsMUX (boot-gates.cpp:34-370).  Synchronous. */
+tfheb_status tfheb_gate_batch(tfheb_cloud_key *ck, int32_t gate, int32_t precision, int32_t count,
+                              const int32_t *a, const int32_t *b, const int32_t *c, int32_t *out);
+
+/* Same on device buffers, enqueued on `stream` (a cudaStream_t, NULL = the key's stream). */
+tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *ck, int32_t gate, int32_t precision, int32_t count,
+                                     const int32_t *d_a, const int32_t *d_b, const int32_t *d_c, int32_t *d_out,
+                                     void *stream);
+
+/* Mixed gate types (gates[count] codes) on device buffers: input i of gate g is row idx_i[g] of the
+ * wire array d_wires ([*][n+1]); outputs go to rows out_idx[g] of d_wires.  Index arrays are host
+ * arrays; they are uploaded once and cached per call site by the netlist API below. */
+tfheb_status tfheb_gate_batch_mixed_device(tfheb_cloud_key *ck, int32_t precision, int32_t count,
+                                           const int32_t *gates, const int32_t *idx_a, const int32_t *idx_b,
+                                           const int32_t *idx_c, const int32_t *out_idx, int32_t *d_wires,
+                                           void *stream);
+
+/* Hot-path pieces on device buffers (the scalar reference functions, batched):
+ *   tfheb_bootstrap_woks_device  -> tfhe_bootstrap_woKS_FFT (lwe-bootstrapping-functions-fft.cpp:169-200)
+ *                                    in [count][n+1] -> out [count][k*N+1]
+ *   tfheb_bootstrap_device       -> tfhe_bootstrap_FFT (lwe-bootstrapping-functions-fft.cpp:213-225)
+ *                                    in [count][n+1] -> out [count][n+1]
+ *   tfheb_blind_rotate_device    -> tfhe_blindRotate_FFT (lwe-bootstrapping-functions-fft.cpp:88-112)
+ *                                    acc [count][k+1][N] in place, bara [count][nsteps] (values in [0,2N))
+ *   tfheb_keyswitch_device       -> lweKeySwitch (lwe-keyswitch-functions.cpp:228-238)
+ *                                    in [count][k*N+1] -> out [count][n+1]                    */
+tfheb_status tfheb_bootstrap_woks_device(tfheb_cloud_key *ck, int32_t precision, int32_t mu, int32_t count,
+                                         const int32_t *d_in, int32_t *d_out, void *stream);
+tfheb_status tfheb_bootstrap_device(tfheb_cloud_key *ck, int32_t precision, int32_t mu, int32_t count,
+                                    const int32_t *d_in, int32_t *d_out, void *stream);
+tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *ck, int32_t precision, int32_t count, int32_t nsteps,
+                                       const int32_t *d_bara, int32_t *d_acc, void *stream);
+tfheb_status tfheb_keyswitch_device(tfheb_cloud_key *ck, int32_t count, const int32_t *d_in, int32_t *d_out,
+                                    void *stream);
+
+/* Synchronise the key's stream and report any pending device error. */
+tfheb_status tfheb_synchronize(tfheb_cloud_key *ck);
+
+/* Layout helpers (host only, no GPU): slot order of the FFT-domain key for ring degree N
+ * (slot_freq[R*N/16]: frequency held by register r of thread t at index r*(N/16)+t). */
+tfheb_status tfheb_fft_slot_order(int32_t N, int32_t *slot_freq);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,7 @@
+"""tfhe_b200: B200-native TFHE gate bootstrapping behind the tfhe v1.1 gate API.
+
+The product is the C-ABI library tfhe_b200/libtfhe_b200.so (include/tfhe_b200.h, include/tfhe.h);
+this package is its Python mirror (tfhe_b200.api)."""
+from . import api  # noqa: F401
+from .api import (FP64, SPLIT_FP32, CloudKey, SecretKey, default_params, fft_slot_order,  # noqa: F401
+                  kernel_launches, keygen, large_params, make_params)

@@ -1,0 +1,231 @@
+"""Python mirror of the engine's C ABI (include/tfhe_b200.h) over ctypes.
+
+Mirrors the reference's gate-bootstrapping interface (tfhe_gate_bootstrapping_functions.h) on raw
+int32 ciphertext arrays: keygen -> encrypt -> batched gates on the GPU -> decrypt.  Torch (or any
+CUDA array with a data pointer) supplies device buffers for the *_device entry points.
+
+The shared library is built in-tree (tfhe_b200/libtfhe_b200.so) by __graft_entry__.build();
+importing this module never falls back to another implementation: if the library is missing,
+loading fails loudly.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtfhe_b200.so")
+
+_V = ctypes.c_void_p
+_I32 = ctypes.c_int32
+
+NAND, OR, AND, XOR, XNOR, NOR, ANDNY, ANDYN, ORNY, ORYN, MUX, NOT, COPY = range(13)
+GATE_NAMES = ["NAND", "OR", "AND", "XOR", "XNOR", "NOR", "ANDNY", "ANDYN", "ORNY", "ORYN", "MUX", "NOT", "COPY"]
+FP64, SPLIT_FP32 = 0, 1
+
+
+class TfhebError(RuntimeError):
+    pass
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("n", _I32), ("N", _I32), ("k", _I32), ("l", _I32), ("Bgbit", _I32), ("ks_t", _I32),
+                ("ks_basebit", _I32), ("ks_stdev", ctypes.c_double), ("bk_stdev", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise TfhebError(f"{LIB_PATH} is missing: build it with __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        L.tfheb_last_error.restype = ctypes.c_char_p
+        L.tfheb_kernel_launches.restype = ctypes.c_int64
+        L.tfheb_keygen.argtypes = [ctypes.POINTER(Params), ctypes.c_uint64, ctypes.POINTER(_V), ctypes.POINTER(_V)]
+        L.tfheb_encrypt.argtypes = [_V, _V, _I32, ctypes.c_uint64, _V]
+        L.tfheb_decrypt.argtypes = [_V, _V, _I32, _V, _V]
+        L.tfheb_cloud_key_to_device.argtypes = [_V, _I32, _I32, _I32]
+        L.tfheb_cloud_key_import.argtypes = [ctypes.POINTER(Params), _V, _V, ctypes.POINTER(_V)]
+        L.tfheb_secret_key_import.argtypes = [ctypes.POINTER(Params), _V, _V, ctypes.POINTER(_V)]
+        L.tfheb_secret_key_export.argtypes = [_V, _V, _V]
+        L.tfheb_cloud_key_export.argtypes = [_V, _V, _V]
+        L.tfheb_secret_key_free.argtypes = [_V]
+        L.tfheb_cloud_key_free.argtypes = [_V]
+        L.tfheb_gate_batch.argtypes = [_V, _I32, _I32, _I32, _V, _V, _V, _V]
+        L.tfheb_gate_batch_device.argtypes = [_V, _I32, _I32, _I32, _V, _V, _V, _V, _V]
+        L.tfheb_bootstrap_woks_device.argtypes = [_V, _I32, _I32, _I32, _V, _V, _V]
+        L.tfheb_bootstrap_device.argtypes = [_V, _I32, _I32, _I32, _V, _V, _V]
+        L.tfheb_blind_rotate_device.argtypes = [_V, _I32, _I32, _I32, _V, _V, _V]
+        L.tfheb_keyswitch_device.argtypes = [_V, _I32, _V, _V, _V]
+        L.tfheb_synchronize.argtypes = [_V]
+        L.tfheb_fft_slot_order.argtypes = [_I32, _V]
+        _lib = L
+    return _lib
+
+
+def _check(status, what):
+    if status != 0:
+        msg = lib().tfheb_last_error().decode(errors="replace")
+        raise TfhebError(f"{what} failed with status {status}: {msg}")
+
+
+def _p(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(_V)
+    return _V(a.data_ptr())  # torch tensor
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def default_params(lam=128):
+    p = Params()
+    _check(lib().tfheb_default_params(lam, ctypes.byref(p)), "tfheb_default_params")
+    return p
+
+
+def large_params():
+    p = Params()
+    _check(lib().tfheb_large_params(ctypes.byref(p)), "tfheb_large_params")
+    return p
+
+
+def make_params(n, N, k, l, Bgbit, ks_t, ks_basebit, ks_stdev=2**-15, bk_stdev=2**-25):
+    return Params(n, N, k, l, Bgbit, ks_t, ks_basebit, ks_stdev, bk_stdev)
+
+
+def kernel_launches():
+    return int(lib().tfheb_kernel_launches())
+
+
+class SecretKey:
+    def __init__(self, handle, params):
+        self.h = _V(handle)
+        self.params = params
+
+    @classmethod
+    def from_raw(cls, params, lwe_key, tlwe_key=None):
+        h = _V()
+        lk = _i32(lwe_key)
+        tk = None if tlwe_key is None else _i32(tlwe_key)
+        _check(lib().tfheb_secret_key_import(ctypes.byref(params), _p(lk), _p(tk), ctypes.byref(h)), "import")
+        return cls(h.value, params)
+
+    def export(self):
+        p = self.params
+        lk = np.zeros(p.n, np.int32)
+        tk = np.zeros(p.k * p.N, np.int32)
+        _check(lib().tfheb_secret_key_export(self.h, _p(lk), _p(tk)), "export")
+        return lk, tk
+
+    def encrypt(self, bits, seed=1):
+        bits = _i32(bits)
+        out = np.zeros((len(bits), self.params.n + 1), np.int32)
+        _check(lib().tfheb_encrypt(self.h, _p(bits), len(bits), seed, _p(out)), "tfheb_encrypt")
+        return out
+
+    def decrypt(self, cts):
+        cts = _i32(cts)
+        bits = np.zeros(len(cts), np.int32)
+        ph = np.zeros(len(cts), np.int32)
+        _check(lib().tfheb_decrypt(self.h, _p(cts), len(cts), _p(bits), _p(ph)), "tfheb_decrypt")
+        return bits, ph
+
+    def free(self):
+        if self.h:
+            lib().tfheb_secret_key_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class CloudKey:
+    """Cloud (evaluation) key: coefficient-domain keys on the host, FFT-domain keys on a GPU."""
+
+    def __init__(self, handle, params):
+        self.h = _V(handle)
+        self.params = params
+
+    @classmethod
+    def from_raw(cls, params, bsk, ksk):
+        h = _V()
+        b, k = _i32(bsk), _i32(ksk)
+        _check(lib().tfheb_cloud_key_import(ctypes.byref(params), _p(b), _p(k), ctypes.byref(h)), "import")
+        return cls(h.value, params)
+
+    def export(self):
+        p = self.params
+        bsk = np.zeros((p.n, (p.k + 1) * p.l, p.k + 1, p.N), np.int32)
+        ksk = np.zeros((p.k * p.N, p.ks_t, 1 << p.ks_basebit, p.n + 1), np.int32)
+        _check(lib().tfheb_cloud_key_export(self.h, _p(bsk), _p(ksk)), "export")
+        return bsk, ksk
+
+    def to_device(self, device=0, precisions=(FP64, SPLIT_FP32), split_shift=0):
+        mask = 0
+        for pr in precisions:
+            mask |= 1 << pr
+        _check(lib().tfheb_cloud_key_to_device(self.h, device, mask, split_shift), "tfheb_cloud_key_to_device")
+        return self
+
+    def gate(self, gate, a, b=None, c=None, precision=FP64):
+        a = _i32(a)
+        b = None if b is None else _i32(b)
+        c = None if c is None else _i32(c)
+        out = np.zeros_like(a)
+        _check(lib().tfheb_gate_batch(self.h, gate, precision, len(a), _p(a), _p(b), _p(c), _p(out)),
+               "tfheb_gate_batch")
+        return out
+
+    def gate_device(self, gate, d_a, d_b, d_c, d_out, count, precision=FP64, stream=None):
+        _check(lib().tfheb_gate_batch_device(self.h, gate, precision, count, _p(d_a), _p(d_b), _p(d_c), _p(d_out),
+                                             stream), "tfheb_gate_batch_device")
+
+    def bootstrap_woks_device(self, d_in, d_out, count, mu, precision=FP64, stream=None):
+        _check(lib().tfheb_bootstrap_woks_device(self.h, precision, mu, count, _p(d_in), _p(d_out), stream),
+               "tfheb_bootstrap_woks_device")
+
+    def blind_rotate_device(self, d_bara, d_acc, count, nsteps, precision=FP64, stream=None):
+        _check(lib().tfheb_blind_rotate_device(self.h, precision, count, nsteps, _p(d_bara), _p(d_acc), stream),
+               "tfheb_blind_rotate_device")
+
+    def keyswitch_device(self, d_in, d_out, count, stream=None):
+        _check(lib().tfheb_keyswitch_device(self.h, count, _p(d_in), _p(d_out), stream), "tfheb_keyswitch_device")
+
+    def synchronize(self):
+        _check(lib().tfheb_synchronize(self.h), "tfheb_synchronize")
+
+    def free(self):
+        if self.h:
+            lib().tfheb_cloud_key_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def keygen(params, seed=1):
+    sk, ck = _V(), _V()
+    _check(lib().tfheb_keygen(ctypes.byref(params), seed, ctypes.byref(sk), ctypes.byref(ck)), "tfheb_keygen")
+    return SecretKey(sk.value, params), CloudKey(ck.value, params)
+
+
+def fft_slot_order(N):
+    out = np.zeros(N // 2, np.int32)
+    _check(lib().tfheb_fft_slot_order(N, _p(out)), "tfheb_fft_slot_order")
+    return out.reshape(8, N // 16)

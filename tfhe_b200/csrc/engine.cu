@@ -1,0 +1,522 @@
+// engine.cu -- C-ABI entry points of libtfhe_b200.so (include/tfhe_b200.h): key lifecycle,
+// device upload, and the batched gate pipeline
+//     prologue -> blind rotation -> extraction -> keyswitch
+// enqueued on one CUDA stream.  No CPU fallback: every gate runs through the kernels.
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+struct tfheb_secret_key {
+    tfheb::SecretKey sk;
+};
+struct tfheb_cloud_key {
+    tfheb::CloudKey ck;
+    std::mutex mu;  // serialises host callers sharing one key (scratch buffers are per key)
+};
+
+namespace tfheb {
+
+static thread_local std::string g_last_error;
+static std::atomic<int64_t> g_launches{0};
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+static tfheb_status cuda_fail(cudaError_t e, const char *where) {
+    set_error(std::string(where) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? TFHEB_ERR_NOMEM : TFHEB_ERR_CUDA;
+}
+
+#define TFHEB_CUDA(call)                                     \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+static bool valid_params(const tfheb_params *p) {
+    if (!p) return false;
+    if (p->n <= 0 || p->N <= 0 || p->k <= 0 || p->l <= 0 || p->Bgbit <= 0 || p->ks_t <= 0 || p->ks_basebit <= 0)
+        return false;
+    if ((p->N & (p->N - 1)) != 0) return false;
+    if (p->l * p->Bgbit > 32 || p->ks_t * p->ks_basebit > 31) return false;
+    return true;
+}
+
+template <typename T>
+static tfheb_status grow(T *&ptr, size_t &cap, size_t need) {
+    if (need <= cap) return TFHEB_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    TFHEB_CUDA(cudaMalloc((void **)&ptr, need * sizeof(T)));
+    cap = need;
+    return TFHEB_OK;
+}
+
+static int bara_stride_of(const tfheb_params &p) { return (p.n + 4) & ~3; }
+
+// gate linear combinations (boot-gates.cpp:34-319): constant numerator/denominator and weights
+struct GateForm {
+    int num, den, sa, sb;
+};
+static const GateForm kForms[10] = {
+    {1, 8, -1, -1},  {1, 8, 1, 1},   {-1, 8, 1, 1},  {1, 4, 2, 2},  {-1, 4, -2, -2},
+    {-1, 8, -1, -1}, {-1, 8, -1, 1}, {-1, 8, 1, -1}, {1, 8, -1, 1}, {1, 8, 1, -1},
+};
+
+// Builds bootstrap and gate descriptors for `count` gates with codes gates[g] (or a uniform code),
+// operands addressed by row indices (or the gate index itself when idx arrays are null).
+static void build_descs(int count, const int32_t *gates, int uniform, const int32_t *ia, const int32_t *ib,
+                        const int32_t *ic, std::vector<BootDesc> &bd, std::vector<GateDesc> &gd,
+                        std::vector<int32_t> *boot_rows) {
+    bd.clear();
+    gd.assign(count, GateDesc{0, -1, 0});
+    (void)ia;
+    (void)ib;
+    (void)ic;
+    (void)boot_rows;
+    const int32_t mu8 = modswitch_to_torus32(1, 8);
+    for (int g = 0; g < count; g++) {
+        const int code = gates ? gates[g] : uniform;
+        if (code == TFHEB_MUX) {
+            const int32_t and_c = modswitch_to_torus32(-1, 8);
+            gd[g].boot0 = (int32_t)bd.size();
+            bd.push_back(BootDesc{g, and_c, 1, 1, 0, 1});   // (0,-1/8) + a + b
+            gd[g].boot1 = (int32_t)bd.size();
+            bd.push_back(BootDesc{g, and_c, -1, 1, 0, 2});  // (0,-1/8) - a + c
+            gd[g].cst = mu8;                                // + (0, 1/8)
+        } else {
+            const GateForm &f = kForms[code];
+            gd[g].boot0 = (int32_t)bd.size();
+            bd.push_back(BootDesc{g, modswitch_to_torus32(f.num, f.den), (int8_t)f.sa, (int8_t)f.sb, 0, 1});
+        }
+    }
+}
+
+static tfheb_status ensure_device(CloudKey &ck, int precision) {
+    if (ck.device < 0) {
+        set_error("cloud key is not on a device (call tfheb_cloud_key_to_device)");
+        return TFHEB_ERR_INVALID;
+    }
+    if (precision != TFHEB_FP64 && precision != TFHEB_SPLIT_FP32) {
+        set_error("unknown precision");
+        return TFHEB_ERR_INVALID;
+    }
+    if (!ck.dbsk[precision].bsk) {
+        set_error("bootstrapping key not prepared for this precision");
+        return TFHEB_ERR_INVALID;
+    }
+    if (!blind_rotate_supported(ck.p)) {
+        set_error("no compiled blind-rotation kernel for this parameter set");
+        return TFHEB_ERR_UNSUPPORTED;
+    }
+    TFHEB_CUDA(cudaSetDevice(ck.device));
+    return TFHEB_OK;
+}
+
+static int default_gpb(const tfheb_params &p, int precision) {
+    (void)precision;
+    return p.N >= 2048 ? 1 : 2;
+}
+
+// Device pipeline for `count` gates described by (bd, gd) already uploaded.
+static tfheb_status run_pipeline(CloudKey &ck, int precision, int count, int boots, const int32_t *d_a,
+                                 const int32_t *d_b, const int32_t *d_c, int32_t *d_out, cudaStream_t s) {
+    const tfheb_params &p = ck.p;
+    const int bs = bara_stride_of(p);
+    const int kN1 = p.k * p.N + 1;
+    tfheb_status st;
+    if ((st = grow(ck.d_bara, ck.bara_cap, (size_t)boots * bs)) != TFHEB_OK) return st;
+    if ((st = grow(ck.d_acc, ck.acc_cap, (size_t)boots * (p.k + 1) * p.N)) != TFHEB_OK) return st;
+    if ((st = grow(ck.d_ksin, ck.ksin_cap, (size_t)count * kN1)) != TFHEB_OK) return st;
+    TFHEB_CUDA(launch_prologue(p, ck.d_bdesc, boots, d_a, d_b, d_c, ck.d_bara, bs, s));
+    TFHEB_CUDA(launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, boots, p.n,
+                                   modswitch_to_torus32(1, 8), nullptr, ck.d_acc, s, default_gpb(p, precision)));
+    TFHEB_CUDA(launch_extract(p, ck.d_gdesc, count, ck.d_acc, ck.d_ksin, kN1, s));
+    TFHEB_CUDA(launch_keyswitch(p, ck.d_ksk, ck.ks_stride, count, ck.d_ksin, kN1, d_out, s));
+    g_launches += 4;
+    ck.launches += 4;
+    return TFHEB_OK;
+}
+
+static tfheb_status upload_descs(CloudKey &ck, const std::vector<BootDesc> &bd, const std::vector<GateDesc> &gd,
+                                 cudaStream_t s) {
+    tfheb_status st;
+    if ((st = grow(ck.d_bdesc, ck.bdesc_cap, bd.size())) != TFHEB_OK) return st;
+    if ((st = grow(ck.d_gdesc, ck.gdesc_cap, gd.size())) != TFHEB_OK) return st;
+    TFHEB_CUDA(cudaMemcpyAsync(ck.d_bdesc, bd.data(), bd.size() * sizeof(BootDesc), cudaMemcpyHostToDevice, s));
+    TFHEB_CUDA(cudaMemcpyAsync(ck.d_gdesc, gd.data(), gd.size() * sizeof(GateDesc), cudaMemcpyHostToDevice, s));
+    TFHEB_CUDA(cudaStreamSynchronize(s));  // host vectors are pageable temporaries
+    return TFHEB_OK;
+}
+
+}  // namespace tfheb
+
+using namespace tfheb;
+
+extern "C" {
+
+const char *tfheb_last_error(void) { return g_last_error.c_str(); }
+
+int64_t tfheb_kernel_launches(void) { return g_launches.load(); }
+
+tfheb_status tfheb_default_params(int32_t lambda, tfheb_params *out) {
+    if (!out || lambda <= 0 || lambda > 128) {
+        set_error("lambda must be in (0, 128] (80-bit and 128-bit sets)");
+        return TFHEB_ERR_INVALID;
+    }
+    if (lambda > 80) *out = tfheb_params{630, 1024, 1, 3, 7, 8, 2, std::pow(2., -15), std::pow(2., -25)};
+    else *out = tfheb_params{500, 1024, 1, 2, 10, 8, 2, 2.44e-5, 7.18e-9};
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_large_params(tfheb_params *out) {
+    if (!out) return TFHEB_ERR_INVALID;
+    *out = tfheb_params{800, 2048, 1, 3, 8, 8, 2, std::pow(2., -15), std::pow(2., -25)};
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_keygen(const tfheb_params *p, uint64_t seed, tfheb_secret_key **sk, tfheb_cloud_key **ck) {
+    if (!valid_params(p) || !sk || !ck) {
+        set_error("invalid parameters");
+        return TFHEB_ERR_INVALID;
+    }
+    auto *s = new tfheb_secret_key();
+    auto *c = new tfheb_cloud_key();
+    keygen(*p, seed, s->sk, c->ck);
+    *sk = s;
+    *ck = c;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_cloud_key_import(const tfheb_params *p, const int32_t *bsk, const int32_t *ksk,
+                                    tfheb_cloud_key **ck) {
+    if (!valid_params(p) || !bsk || !ksk || !ck) {
+        set_error("invalid arguments");
+        return TFHEB_ERR_INVALID;
+    }
+    auto *c = new tfheb_cloud_key();
+    c->ck.p = *p;
+    const size_t nb = (size_t)p->n * (p->k + 1) * p->l * (p->k + 1) * p->N;
+    const size_t nk = (size_t)p->k * p->N * p->ks_t * (1 << p->ks_basebit) * (p->n + 1);
+    c->ck.bsk_coef.assign(bsk, bsk + nb);
+    c->ck.ksk.assign(ksk, ksk + nk);
+    *ck = c;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_secret_key_import(const tfheb_params *p, const int32_t *lwe_key, const int32_t *tlwe_key,
+                                     tfheb_secret_key **sk) {
+    if (!valid_params(p) || !lwe_key || !sk) {
+        set_error("invalid arguments");
+        return TFHEB_ERR_INVALID;
+    }
+    auto *s = new tfheb_secret_key();
+    s->sk.p = *p;
+    s->sk.lwe_key.assign(lwe_key, lwe_key + p->n);
+    if (tlwe_key) s->sk.tlwe_key.assign(tlwe_key, tlwe_key + (size_t)p->k * p->N);
+    *sk = s;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_secret_key_export(const tfheb_secret_key *sk, int32_t *lwe_key, int32_t *tlwe_key) {
+    if (!sk) return TFHEB_ERR_INVALID;
+    if (lwe_key) std::memcpy(lwe_key, sk->sk.lwe_key.data(), sk->sk.lwe_key.size() * 4);
+    if (tlwe_key) std::memcpy(tlwe_key, sk->sk.tlwe_key.data(), sk->sk.tlwe_key.size() * 4);
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_cloud_key_export(const tfheb_cloud_key *ck, int32_t *bsk, int32_t *ksk) {
+    if (!ck) return TFHEB_ERR_INVALID;
+    if (bsk) std::memcpy(bsk, ck->ck.bsk_coef.data(), ck->ck.bsk_coef.size() * 4);
+    if (ksk) std::memcpy(ksk, ck->ck.ksk.data(), ck->ck.ksk.size() * 4);
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_cloud_key_params(const tfheb_cloud_key *ck, tfheb_params *out) {
+    if (!ck || !out) return TFHEB_ERR_INVALID;
+    *out = ck->ck.p;
+    return TFHEB_OK;
+}
+
+void tfheb_secret_key_free(tfheb_secret_key *sk) { delete sk; }
+
+void tfheb_cloud_key_free(tfheb_cloud_key *c) {
+    if (!c) return;
+    CloudKey &ck = c->ck;
+    if (ck.device >= 0) {
+        cudaSetDevice(ck.device);
+        for (auto &d : ck.dbsk) {
+            cudaFree(d.bsk);
+            cudaFree(d.tables);
+        }
+        cudaFree(ck.d_ksk);
+        cudaFree(ck.d_bara);
+        cudaFree(ck.d_acc);
+        cudaFree(ck.d_ksin);
+        cudaFree(ck.d_io);
+        cudaFree(ck.d_bdesc);
+        cudaFree(ck.d_gdesc);
+        cudaFree(ck.d_err);
+        if (ck.h_io) cudaFreeHost(ck.h_io);
+        if (ck.stream) cudaStreamDestroy(ck.stream);
+    }
+    delete c;
+}
+
+tfheb_status tfheb_encrypt(const tfheb_secret_key *sk, const int32_t *bits, int32_t count, uint64_t seed,
+                           int32_t *out) {
+    if (!sk || !bits || !out || count < 0) return TFHEB_ERR_INVALID;
+    encrypt(sk->sk, bits, count, seed, out);
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_decrypt(const tfheb_secret_key *sk, const int32_t *cts, int32_t count, int32_t *bits,
+                           int32_t *phases) {
+    if (!sk || !cts || count < 0) return TFHEB_ERR_INVALID;
+    const int n = sk->sk.p.n;
+    for (int g = 0; g < count; g++) {
+        const int32_t ph = phase(sk->sk, cts + (size_t)g * (n + 1));
+        if (bits) bits[g] = ph > 0 ? 1 : 0;  // tfhe_gate_bootstrapping.cpp:162-165
+        if (phases) phases[g] = ph;
+    }
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32_t precision_mask,
+                                       int32_t split_shift) {
+    if (!c) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        set_error("no CUDA device visible");
+        return TFHEB_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev || (ck.device >= 0 && ck.device != device)) return TFHEB_ERR_INVALID;
+    if (!blind_rotate_supported(ck.p)) {
+        set_error("no compiled blind-rotation kernel for this parameter set");
+        return TFHEB_ERR_UNSUPPORTED;
+    }
+    if (split_shift == 0) split_shift = 24;
+    if (split_shift < 8 || split_shift > 30) return TFHEB_ERR_INVALID;
+    TFHEB_CUDA(cudaSetDevice(device));
+    ck.device = device;
+    if (!ck.stream) TFHEB_CUDA(cudaStreamCreateWithFlags(&ck.stream, cudaStreamNonBlocking));
+    const tfheb_params &p = ck.p;
+    // keyswitching key, rows padded to a multiple of 4 int32 (16-byte aligned vector loads)
+    if (!ck.d_ksk) {
+        ck.ks_stride = (p.n + 1 + 3) & ~3;
+        const size_t rows = (size_t)p.k * p.N * p.ks_t * (1 << p.ks_basebit);
+        std::vector<int32_t> padded(rows * ck.ks_stride, 0);
+        for (size_t r = 0; r < rows; r++)
+            std::memcpy(&padded[r * ck.ks_stride], &ck.ksk[r * (p.n + 1)], (p.n + 1) * 4);
+        TFHEB_CUDA(cudaMalloc((void **)&ck.d_ksk, padded.size() * 4));
+        TFHEB_CUDA(cudaMemcpy(ck.d_ksk, padded.data(), padded.size() * 4, cudaMemcpyHostToDevice));
+    }
+    std::vector<double> tab;
+    build_tables_fp64(p.N, tab);
+    for (int prec = 0; prec < 2; prec++) {
+        if (!(precision_mask & (1 << prec))) continue;
+        DeviceBsk &d = ck.dbsk[prec];
+        if (d.bsk && (prec == TFHEB_FP64 || d.split_shift == split_shift)) continue;
+        if (d.bsk) {
+            cudaFree(d.bsk);
+            cudaFree(d.tables);
+            d.bsk = d.tables = nullptr;
+        }
+        std::vector<uint8_t> fbsk;
+        transform_bsk(p, ck.bsk_coef.data(), prec, split_shift, fbsk);
+        TFHEB_CUDA(cudaMalloc(&d.bsk, fbsk.size()));
+        TFHEB_CUDA(cudaMemcpy(d.bsk, fbsk.data(), fbsk.size(), cudaMemcpyHostToDevice));
+        d.bsk_bytes = fbsk.size();
+        d.split_shift = prec == TFHEB_SPLIT_FP32 ? split_shift : 0;
+        if (prec == TFHEB_FP64) {
+            TFHEB_CUDA(cudaMalloc(&d.tables, tab.size() * sizeof(double)));
+            TFHEB_CUDA(cudaMemcpy(d.tables, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+        } else {
+            std::vector<float> tf(tab.begin(), tab.end());
+            TFHEB_CUDA(cudaMalloc(&d.tables, tf.size() * sizeof(float)));
+            TFHEB_CUDA(cudaMemcpy(d.tables, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice));
+        }
+    }
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *c, int32_t gate, int32_t precision, int32_t count,
+                                     const int32_t *d_a, const int32_t *d_b, const int32_t *d_c, int32_t *d_out,
+                                     void *stream) {
+    if (!c || count < 0 || gate < 0 || gate > TFHEB_COPY || !d_a || !d_out) return TFHEB_ERR_INVALID;
+    if (gate == TFHEB_MUX && (!d_b || !d_c)) return TFHEB_ERR_INVALID;
+    if (gate < TFHEB_MUX && !d_b) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    tfheb_status st = ensure_device(ck, precision);
+    if (st != TFHEB_OK) return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+    if (count == 0) return TFHEB_OK;
+    const int n1 = ck.p.n + 1;
+    if (gate == TFHEB_COPY || gate == TFHEB_NOT) {
+        // bootstrap-free (boot-gates.cpp:164-178)
+        if (gate == TFHEB_COPY) {
+            TFHEB_CUDA(cudaMemcpyAsync(d_out, d_a, (size_t)count * n1 * 4, cudaMemcpyDeviceToDevice, s));
+            return TFHEB_OK;
+        }
+        TFHEB_CUDA(launch_negate(d_a, d_out, (size_t)count * n1, s));
+        g_launches += 1;
+        return TFHEB_OK;
+    }
+    if (ck.cached_gate != gate || ck.cached_count != count) {
+        std::vector<BootDesc> bd;
+        std::vector<GateDesc> gd;
+        build_descs(count, nullptr, gate, nullptr, nullptr, nullptr, bd, gd, nullptr);
+        if ((st = upload_descs(ck, bd, gd, s)) != TFHEB_OK) return st;
+        ck.cached_gate = gate;
+        ck.cached_count = count;
+    }
+    const int boots = gate == TFHEB_MUX ? 2 * count : count;
+    return run_pipeline(ck, precision, count, boots, d_a, d_b, d_c, d_out, s);
+}
+
+tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precision, int32_t count,
+                              const int32_t *a, const int32_t *b, const int32_t *cc, int32_t *out) {
+    if (!c || count < 0 || !a || !out) return TFHEB_ERR_INVALID;
+    if (count == 0) return TFHEB_OK;
+    CloudKey &ck = c->ck;
+    if (ck.device < 0) {
+        set_error("cloud key is not on a device (call tfheb_cloud_key_to_device)");
+        return TFHEB_ERR_INVALID;
+    }
+    const size_t row = (size_t)ck.p.n + 1, sz = (size_t)count * row;
+    int32_t *dio;
+    {
+        std::lock_guard<std::mutex> lock(c->mu);
+        TFHEB_CUDA(cudaSetDevice(ck.device));
+        tfheb_status st = grow(ck.d_io, ck.io_cap, 4 * sz);
+        if (st != TFHEB_OK) return st;
+        dio = ck.d_io;
+        cudaStream_t s = ck.stream;
+        TFHEB_CUDA(cudaMemcpyAsync(dio, a, sz * 4, cudaMemcpyHostToDevice, s));
+        if (b) TFHEB_CUDA(cudaMemcpyAsync(dio + sz, b, sz * 4, cudaMemcpyHostToDevice, s));
+        if (cc) TFHEB_CUDA(cudaMemcpyAsync(dio + 2 * sz, cc, sz * 4, cudaMemcpyHostToDevice, s));
+    }
+    tfheb_status st = tfheb_gate_batch_device(c, gate, precision, count, dio, b ? dio + sz : nullptr,
+                                              cc ? dio + 2 * sz : nullptr, dio + 3 * sz, nullptr);
+    if (st != TFHEB_OK) return st;
+    std::lock_guard<std::mutex> lock(c->mu);
+    TFHEB_CUDA(cudaMemcpyAsync(out, dio + 3 * sz, sz * 4, cudaMemcpyDeviceToHost, ck.stream));
+    TFHEB_CUDA(cudaStreamSynchronize(ck.stream));
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_gate_batch_mixed_device(tfheb_cloud_key *c, int32_t precision, int32_t count, const int32_t *gates,
+                                           const int32_t *idx_a, const int32_t *idx_b, const int32_t *idx_c,
+                                           const int32_t *out_idx, int32_t *d_wires, void *stream) {
+    (void)c; (void)precision; (void)count; (void)gates; (void)idx_a; (void)idx_b; (void)idx_c; (void)out_idx;
+    (void)d_wires; (void)stream;
+    set_error("mixed batches are evaluated through the netlist API");
+    return TFHEB_ERR_UNSUPPORTED;
+}
+
+tfheb_status tfheb_bootstrap_woks_device(tfheb_cloud_key *c, int32_t precision, int32_t mu, int32_t count,
+                                         const int32_t *d_in, int32_t *d_out, void *stream) {
+    if (!c || count < 0 || !d_in || !d_out) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    tfheb_status st = ensure_device(ck, precision);
+    if (st != TFHEB_OK) return st;
+    if (count == 0) return TFHEB_OK;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+    const tfheb_params &p = ck.p;
+    // identity combination: x = in, one bootstrap per sample, no MUX term
+    std::vector<BootDesc> bd(count);
+    std::vector<GateDesc> gd(count);
+    for (int g = 0; g < count; g++) {
+        bd[g] = BootDesc{g, 0, 1, 0, 0, 0};
+        gd[g] = GateDesc{g, -1, 0};
+    }
+    if ((st = upload_descs(ck, bd, gd, s)) != TFHEB_OK) return st;
+    ck.cached_gate = ck.cached_count = -1;
+    const int bs = bara_stride_of(p);
+    if ((st = grow(ck.d_bara, ck.bara_cap, (size_t)count * bs)) != TFHEB_OK) return st;
+    if ((st = grow(ck.d_acc, ck.acc_cap, (size_t)count * (p.k + 1) * p.N)) != TFHEB_OK) return st;
+    TFHEB_CUDA(launch_prologue(p, ck.d_bdesc, count, d_in, d_in, d_in, ck.d_bara, bs, s));
+    TFHEB_CUDA(launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, count, p.n, mu, nullptr,
+                                   ck.d_acc, s, default_gpb(p, precision)));
+    TFHEB_CUDA(launch_extract(p, ck.d_gdesc, count, ck.d_acc, d_out, p.k * p.N + 1, s));
+    g_launches += 3;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_bootstrap_device(tfheb_cloud_key *c, int32_t precision, int32_t mu, int32_t count,
+                                    const int32_t *d_in, int32_t *d_out, void *stream) {
+    if (!c || count < 0 || !d_in || !d_out) return TFHEB_ERR_INVALID;
+    CloudKey &ck = c->ck;
+    int32_t *tmp;
+    {
+        std::lock_guard<std::mutex> lock(c->mu);
+        if (ck.device < 0) return TFHEB_ERR_INVALID;
+        TFHEB_CUDA(cudaSetDevice(ck.device));
+        tfheb_status st = grow(ck.d_ksin, ck.ksin_cap, (size_t)count * (ck.p.k * ck.p.N + 1));
+        if (st != TFHEB_OK) return st;
+        tmp = ck.d_ksin;
+    }
+    tfheb_status st = tfheb_bootstrap_woks_device(c, precision, mu, count, d_in, tmp, stream);
+    if (st != TFHEB_OK) return st;
+    return tfheb_keyswitch_device(c, count, tmp, d_out, stream);
+}
+
+tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *c, int32_t precision, int32_t count, int32_t nsteps,
+                                       const int32_t *d_bara, int32_t *d_acc, void *stream) {
+    if (!c || count < 0 || !d_bara || !d_acc || nsteps < 0) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    if (nsteps > ck.p.n) return TFHEB_ERR_INVALID;
+    tfheb_status st = ensure_device(ck, precision);
+    if (st != TFHEB_OK) return st;
+    if (count == 0) return TFHEB_OK;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+    // in place: acc_in == acc_out is safe (each team reads its row fully before writing it back)
+    TFHEB_CUDA(launch_blind_rotate(ck.p, precision, ck.dbsk[precision], d_bara, nsteps, count, nsteps, 0, d_acc,
+                                   d_acc, s, default_gpb(ck.p, precision)));
+    g_launches += 1;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_keyswitch_device(tfheb_cloud_key *c, int32_t count, const int32_t *d_in, int32_t *d_out,
+                                    void *stream) {
+    if (!c || count < 0 || !d_in || !d_out) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    if (ck.device < 0 || !ck.d_ksk) return TFHEB_ERR_INVALID;
+    TFHEB_CUDA(cudaSetDevice(ck.device));
+    if (count == 0) return TFHEB_OK;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+    TFHEB_CUDA(launch_keyswitch(ck.p, ck.d_ksk, ck.ks_stride, count, d_in, ck.p.k * ck.p.N + 1, d_out, s));
+    g_launches += 1;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_synchronize(tfheb_cloud_key *c) {
+    if (!c) return TFHEB_ERR_INVALID;
+    CloudKey &ck = c->ck;
+    if (ck.device < 0) return TFHEB_OK;
+    TFHEB_CUDA(cudaSetDevice(ck.device));
+    TFHEB_CUDA(cudaStreamSynchronize(ck.stream));
+    TFHEB_CUDA(cudaGetLastError());
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_fft_slot_order(int32_t N, int32_t *slot_freq) {
+    std::vector<int32_t> sf;
+    fill_slot_freq(N, sf);
+    if (sf.empty() || !slot_freq) return TFHEB_ERR_UNSUPPORTED;
+    std::memcpy(slot_freq, sf.data(), sf.size() * 4);
+    return TFHEB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,278 @@
+// fft.cuh -- negacyclic FFT building blocks for the blind-rotation kernel (sm_100a).
+//
+// A real polynomial a of degree < N in R[X]/(X^N+1) is folded into M = N/2 complex points
+//     z_j = (a_j - i a_{j+M}) * exp(-i pi j / N),   j < M,
+// and a size-M complex DFT with W = exp(-2 pi i / M) then evaluates a at the M primitive 2N-th
+// roots exp(-i pi (4k+1) / N); products in the ring become pointwise products.  This is the same
+// "half-size complex" representation the reference keeps in LagrangeHalfCPolynomial
+// (fft_processors/spqlios/lagrangehalfc_impl.h:40-45), derived and laid out independently here.
+//
+// One FFT is computed by a team of T = M/R threads holding R = 8 points each in registers.
+// The transform is an in-place mixed-radix decimation-in-frequency over the stage radices of
+// FftPlan<M>; between stages the team exchanges points through shared memory.  The forward
+// transform leaves the spectrum in "slot order" (thread t, register r) = digit-reversed frequency,
+// so no reordering pass exists: the bootstrapping key is stored in the same slot order by the host,
+// the multiply-accumulate is pointwise on registers, and the inverse transform (the exact adjoint
+// of the forward stages) consumes slot order and returns natural order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tfheb {
+
+template <typename T>
+struct cplx {
+    T re, im;
+};
+
+template <typename T>
+__device__ __forceinline__ cplx<T> cadd(cplx<T> a, cplx<T> b) { return {a.re + b.re, a.im + b.im}; }
+template <typename T>
+__device__ __forceinline__ cplx<T> csub(cplx<T> a, cplx<T> b) { return {a.re - b.re, a.im - b.im}; }
+template <typename T>
+__device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b) {
+    return {fma(a.re, b.re, -a.im * b.im), fma(a.re, b.im, a.im * b.re)};
+}
+template <typename T>
+__device__ __forceinline__ cplx<T> cmulconj(cplx<T> a, cplx<T> b) {  // a * conj(b)
+    return {fma(a.re, b.re, a.im * b.im), fma(a.im, b.re, -a.re * b.im)};
+}
+// acc += a * b
+template <typename T>
+__device__ __forceinline__ void cmac(cplx<T> &acc, cplx<T> a, cplx<T> b) {
+    acc.re = fma(a.re, b.re, acc.re);
+    acc.re = fma(-a.im, b.im, acc.re);
+    acc.im = fma(a.re, b.im, acc.im);
+    acc.im = fma(a.im, b.re, acc.im);
+}
+
+// multiply by -i (forward) or +i (inverse)
+template <typename T, bool INV>
+__device__ __forceinline__ cplx<T> rot_quarter(cplx<T> a) {
+    if (INV) return {-a.im, a.re};
+    return {a.im, -a.re};
+}
+
+template <typename T>
+__device__ __forceinline__ T rsqrt2() { return T(0.70710678118654752440084436210485); }
+
+// ---- small DFT codelets: natural-order input and output, W_r = exp(-2 pi i / r) (conj if INV) --
+
+template <typename T, bool INV>
+__device__ __forceinline__ void dft2(cplx<T> *x) {
+    const cplx<T> a = x[0], b = x[1];
+    x[0] = cadd(a, b);
+    x[1] = csub(a, b);
+}
+
+template <typename T, bool INV>
+__device__ __forceinline__ void dft4(cplx<T> &x0, cplx<T> &x1, cplx<T> &x2, cplx<T> &x3) {
+    const cplx<T> s02 = cadd(x0, x2), d02 = csub(x0, x2);
+    const cplx<T> s13 = cadd(x1, x3), d13 = rot_quarter<T, INV>(csub(x1, x3));
+    x0 = cadd(s02, s13);
+    x2 = csub(s02, s13);
+    x1 = cadd(d02, d13);
+    x3 = csub(d02, d13);
+}
+
+template <typename T, bool INV>
+__device__ __forceinline__ void dft4(cplx<T> *x) { dft4<T, INV>(x[0], x[1], x[2], x[3]); }
+
+template <typename T, bool INV>
+__device__ __forceinline__ void dft8(cplx<T> *x) {
+    cplx<T> e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6];
+    cplx<T> o0 = x[1], o1 = x[3], o2 = x[5], o3 = x[7];
+    dft4<T, INV>(e0, e1, e2, e3);
+    dft4<T, INV>(o0, o1, o2, o3);
+    const T h = rsqrt2<T>();
+    // o_k *= W8^k (forward W8 = (1-i)/sqrt2; inverse uses the conjugate)
+    cplx<T> w1, w3;
+    if (!INV) {
+        w1 = {(o1.re + o1.im) * h, (o1.im - o1.re) * h};
+        w3 = {(o3.im - o3.re) * h, -(o3.re + o3.im) * h};
+    } else {
+        w1 = {(o1.re - o1.im) * h, (o1.re + o1.im) * h};
+        w3 = {-(o3.re + o3.im) * h, (o3.re - o3.im) * h};
+    }
+    const cplx<T> w2 = rot_quarter<T, INV>(o2);
+    x[0] = cadd(e0, o0);
+    x[4] = csub(e0, o0);
+    x[1] = cadd(e1, w1);
+    x[5] = csub(e1, w1);
+    x[2] = cadd(e2, w2);
+    x[6] = csub(e2, w2);
+    x[3] = cadd(e3, w3);
+    x[7] = csub(e3, w3);
+}
+
+template <typename T, bool INV, int RADIX>
+__device__ __forceinline__ void dft(cplx<T> *x) {
+    if constexpr (RADIX == 8) dft8<T, INV>(x);
+    else if constexpr (RADIX == 4) dft4<T, INV>(x);
+    else dft2<T, INV>(x);
+}
+
+// ---- plans -----------------------------------------------------------------------------------
+// Stage radices per transform size (R = 8 points per thread): every radix divides R.
+
+template <int M>
+struct FftPlan;
+template <>
+struct FftPlan<64> {
+    static constexpr int NS = 2;
+    __host__ __device__ static constexpr int radix(int) { return 8; }
+};
+template <>
+struct FftPlan<256> {
+    static constexpr int NS = 3;
+    __host__ __device__ static constexpr int radix(int s) { return s < 2 ? 8 : 4; }
+};
+template <>
+struct FftPlan<512> {
+    static constexpr int NS = 3;
+    __host__ __device__ static constexpr int radix(int) { return 8; }
+};
+template <>
+struct FftPlan<1024> {
+    static constexpr int NS = 4;
+    __host__ __device__ static constexpr int radix(int s) { return s < 3 ? 8 : 2; }
+};
+
+// sub-transform length entering stage S
+template <int M>
+__host__ __device__ constexpr int stage_len(int S) {
+    int L = M;
+    for (int s = 0; s < S; s++) L /= FftPlan<M>::radix(s);
+    return L;
+}
+
+template <int M, int S>
+struct Stage {
+    static constexpr int r = FftPlan<M>::radix(S);
+    static constexpr int L = stage_len<M>(S);
+    static constexpr int stride = L / r;
+};
+
+// Stage S stores W_L^{n1*k2} at [(k2-1)*stride + n1] (k2 in [1,r), n1 < stride), packed in order.
+template <int M>
+__host__ __device__ constexpr int tw_offset(int S) {
+    int off = 0;
+    for (int s = 0; s < S; s++) {
+        const int L = stage_len<M>(s), r = FftPlan<M>::radix(s);
+        off += (r - 1) * (L / r);
+    }
+    return off;
+}
+// Shared-memory swizzle for the exchange buffer (bank-conflict free for the FP32 patterns).
+__device__ __forceinline__ int swz(int p) { return p ^ ((p >> 3) & 31); }
+
+// Named barrier over one team (ids 1..15; 0 is __syncthreads).
+__device__ __forceinline__ void team_sync(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Team FFT: T = M/R threads, t in [0,T), registers x[R], exchange buffer buf_re/buf_im (M entries).
+template <typename T, int M, int R>
+struct TeamFft {
+    static constexpr int NT = M / R;  // threads per team
+    static constexpr int NS = FftPlan<M>::NS;
+
+    // position of register (c, n2) of thread t at stage S
+    template <int S>
+    __device__ static __forceinline__ int pos(int t, int c, int n2) {
+        constexpr int r = Stage<M, S>::r, L = Stage<M, S>::L, st = Stage<M, S>::stride;
+        const int b = t + NT * c;
+        const int q = b / st, n1 = b - q * st;
+        return q * L + n1 + st * n2;
+    }
+
+    template <int S>
+    __device__ static __forceinline__ void store(const cplx<T> *x, T *buf_re, T *buf_im, int t) {
+        constexpr int r = Stage<M, S>::r;
+#pragma unroll
+        for (int c = 0; c < R / r; c++)
+#pragma unroll
+            for (int n2 = 0; n2 < r; n2++) {
+                const int p = swz(pos<S>(t, c, n2));
+                buf_re[p] = x[c * r + n2].re;
+                buf_im[p] = x[c * r + n2].im;
+            }
+    }
+
+    template <int S>
+    __device__ static __forceinline__ void load(cplx<T> *x, const T *buf_re, const T *buf_im, int t) {
+        constexpr int r = Stage<M, S>::r;
+#pragma unroll
+        for (int c = 0; c < R / r; c++)
+#pragma unroll
+            for (int n2 = 0; n2 < r; n2++) {
+                const int p = swz(pos<S>(t, c, n2));
+                x[c * r + n2].re = buf_re[p];
+                x[c * r + n2].im = buf_im[p];
+            }
+    }
+
+    template <int S, bool INV>
+    __device__ static __forceinline__ void twiddle(cplx<T> *x, const cplx<T> *tw, int t) {
+        constexpr int r = Stage<M, S>::r, st = Stage<M, S>::stride;
+        if constexpr (st > 1) {
+            const cplx<T> *tws = tw + tw_offset<M>(S);
+#pragma unroll
+            for (int c = 0; c < R / r; c++) {
+                const int b = t + NT * c;
+                const int n1 = b % st;
+#pragma unroll
+                for (int k2 = 1; k2 < r; k2++) {
+                    const cplx<T> w = tws[(k2 - 1) * st + n1];
+                    x[c * r + k2] = INV ? cmulconj(x[c * r + k2], w) : cmul(x[c * r + k2], w);
+                }
+            }
+        }
+    }
+
+    template <int S>
+    __device__ static __forceinline__ void forward_from(cplx<T> *x, T *buf_re, T *buf_im, const cplx<T> *tw,
+                                                        int t, int bar_id) {
+        constexpr int r = Stage<M, S>::r;
+#pragma unroll
+        for (int c = 0; c < R / r; c++) dft<T, false, r>(x + c * r);
+        twiddle<S, false>(x, tw, t);
+        if constexpr (S + 1 < NS) {
+            store<S>(x, buf_re, buf_im, t);
+            team_sync(bar_id, NT);
+            load<S + 1>(x, buf_re, buf_im, t);
+            team_sync(bar_id, NT);
+            forward_from<S + 1>(x, buf_re, buf_im, tw, t, bar_id);
+        }
+    }
+
+    template <int S>
+    __device__ static __forceinline__ void inverse_from(cplx<T> *x, T *buf_re, T *buf_im, const cplx<T> *tw,
+                                                        int t, int bar_id) {
+        constexpr int r = Stage<M, S>::r;
+        twiddle<S, true>(x, tw, t);
+#pragma unroll
+        for (int c = 0; c < R / r; c++) dft<T, true, r>(x + c * r);
+        if constexpr (S > 0) {
+            store<S>(x, buf_re, buf_im, t);
+            team_sync(bar_id, NT);
+            load<S - 1>(x, buf_re, buf_im, t);
+            team_sync(bar_id, NT);
+            inverse_from<S - 1>(x, buf_re, buf_im, tw, t, bar_id);
+        }
+    }
+
+    // natural order in (x[n2] = point t + NT*n2) -> slot order out
+    __device__ static __forceinline__ void forward(cplx<T> *x, T *buf_re, T *buf_im, const cplx<T> *tw, int t,
+                                                   int bar_id) {
+        forward_from<0>(x, buf_re, buf_im, tw, t, bar_id);
+    }
+    // slot order in -> natural order out (unscaled: returns M * the inverse DFT)
+    __device__ static __forceinline__ void inverse(cplx<T> *x, T *buf_re, T *buf_im, const cplx<T> *tw, int t,
+                                                   int bar_id) {
+        inverse_from<NS - 1>(x, buf_re, buf_im, tw, t, bar_id);
+    }
+};
+
+}  // namespace tfheb

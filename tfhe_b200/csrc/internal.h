@@ -1,0 +1,105 @@
+// internal.h -- shared declarations of the tfhe_b200 engine (host runtime + kernel launchers).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/tfhe_b200.h"
+
+namespace tfheb {
+
+constexpr int kR = 8;  // FFT points per thread
+
+// Per-bootstrap descriptor: which inputs the gate's linear combination reads and with what weights
+// (boot-gates.cpp:34-370).  x/y select the operand: 0 = a, 1 = b, 2 = c.
+struct BootDesc {
+    int32_t gate;  // gate (output) index
+    int32_t cst;   // Torus32 constant added to b
+    int8_t sa, sb; // integer weights of operands x and y
+    uint8_t xsel, ysel;
+};
+
+// Per-gate descriptor for the extraction stage: output = extract(acc[boot0]) (+ extract(acc[boot1]))
+// + (0, cst).  boot1 < 0 for one-bootstrap gates.
+struct GateDesc {
+    int32_t boot0, boot1;
+    int32_t cst;
+};
+
+// Device-side FFT-domain bootstrapping key and tables for one precision.
+struct DeviceBsk {
+    void *bsk = nullptr;      // [n][kpl][k+1][R][NT] x 16 bytes (double2, or float4 = hi.re,hi.im,lo.re,lo.im)
+    void *tables = nullptr;   // stage twiddles followed by the twist table [R][NT]
+    size_t bsk_bytes = 0;
+    int split_shift = 0;      // split mode: weight of the high limb is 2^split_shift
+};
+
+struct CloudKey {
+    tfheb_params p{};
+    std::vector<int32_t> bsk_coef;  // [n][kpl][k+1][N] coefficient domain (host)
+    std::vector<int32_t> ksk;       // [kN][t][base][n+1] (host)
+    // device state
+    int device = -1;
+    DeviceBsk dbsk[2];              // [TFHEB_FP64], [TFHEB_SPLIT_FP32]
+    int32_t *d_ksk = nullptr;       // [kN][t][base][ks_stride]
+    int ks_stride = 0;              // padded row length (multiple of 4 >= n+1)
+    cudaStream_t stream = nullptr;
+    // scratch (grown on demand)
+    int32_t *d_bara = nullptr;
+    size_t bara_cap = 0;
+    int32_t *d_acc = nullptr;
+    size_t acc_cap = 0;
+    int32_t *d_ksin = nullptr;
+    size_t ksin_cap = 0;
+    int32_t *d_io = nullptr;        // staging of host batches: a,b,c,out
+    size_t io_cap = 0;
+    int32_t *h_io = nullptr;        // pinned host staging
+    size_t h_io_cap = 0;
+    BootDesc *d_bdesc = nullptr;
+    size_t bdesc_cap = 0;
+    GateDesc *d_gdesc = nullptr;
+    size_t gdesc_cap = 0;
+    int cached_gate = -1, cached_count = -1;
+    int32_t *d_err = nullptr;       // device error word
+    int launches = 0;               // kernels launched (for the bench's launch count)
+};
+
+struct SecretKey {
+    tfheb_params p{};
+    std::vector<int32_t> lwe_key;   // [n]
+    std::vector<int32_t> tlwe_key;  // [k][N]
+};
+
+// ---- host helpers (host_keys.cu) ------------------------------------------------------------
+void keygen(const tfheb_params &p, uint64_t seed, SecretKey &sk, CloudKey &ck);
+void encrypt(const SecretKey &sk, const int32_t *bits, int32_t count, uint64_t seed, int32_t *out);
+int32_t phase(const SecretKey &sk, const int32_t *ct);
+int32_t modswitch_to_torus32(int32_t mu, int32_t msize);
+int32_t modswitch_from_torus32(int32_t phase, int32_t msize);
+
+// FFT-domain key preparation (host FP64), layout-compatible with the kernels.
+void build_tables_fp64(int N, std::vector<double> &tables);  // complex pairs (re,im)
+void fill_slot_freq(int N, std::vector<int32_t> &slot_freq); // [R][NT] -> frequency index
+void transform_bsk(const tfheb_params &p, const int32_t *bsk_coef, int precision, int split_shift,
+                   std::vector<uint8_t> &out);
+
+// ---- kernel launchers (kernels.cu) ----------------------------------------------------------
+cudaError_t launch_prologue(const tfheb_params &p, const BootDesc *d_desc, int boots, const int32_t *a,
+                            const int32_t *b, const int32_t *c, int32_t *bara, int bara_stride, cudaStream_t s);
+cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const DeviceBsk &bsk, const int32_t *bara,
+                                int bara_stride, int boots, int nsteps, int32_t mu, const int32_t *acc_in,
+                                int32_t *acc_out, cudaStream_t s, int gates_per_cta);
+cudaError_t launch_extract(const tfheb_params &p, const GateDesc *d_desc, int count, const int32_t *acc,
+                           int32_t *out, int out_stride, cudaStream_t s);
+cudaError_t launch_keyswitch(const tfheb_params &p, const int32_t *d_ksk, int ks_stride, int count,
+                             const int32_t *in, int in_stride, int32_t *out, cudaStream_t s);
+int blind_rotate_supported(const tfheb_params &p);
+cudaError_t launch_negate(const int32_t *in, int32_t *out, size_t count, cudaStream_t s);
+
+// ---- errors ---------------------------------------------------------------------------------
+void set_error(const std::string &msg);
+
+}  // namespace tfheb
