@@ -1,0 +1,324 @@
+"""Benchmark of the gate-bootstrapping hot path on B200.
+
+Workload (one "step"): 4096 independent bootsNAND gates in one batch at the default 128-bit
+parameters (n=630, N=1024, k=1, l=3, Bgbit=7, ks t=8 basebit=2): gate prologue + mod-switch,
+blind rotation (630 CMUX steps), sample extraction and keyswitch, on GPU-resident ciphertexts.
+The headline `value` is the split-FP32 form; the plain FP64 form is measured in the same run
+(`fp64`).  Multi-GPU runs are independent replicas (one key set per GPU, no collective on the data
+path); value = all gates of all ranks / the slowest rank's device time.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--form split|fp64]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "bootstrapped gates/s on 1 B200: split-FP32 vs FP64 FFT, 0 errors in 1e6 gates"
+UNIT = "gates/s"
+PARAMS = "n=630,N=1024,k=1,l=3,Bgbit=7,ks_t=8,ks_basebit=2"
+
+# Algorithmic work per gate (FFT of size M complex = 5 M log2 M flops, twist 6M, complex MAC 8):
+# per CMUX step FP64 = 8 transforms + 12*512 MACs = 258,048 flops; split = 10 transforms + 24*512 MACs
+# = 359,424 flops; x 630 steps.
+FLOPS_PER_GATE = {"fp64": 162.57e6, "split": 226.44e6}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--form", choices=["split", "fp64"], default="split")
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=5)
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        under_load = [s for s in sm if s > 0.3 * max(sm)] if sm else []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(under_load) if under_load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(seconds, batch_hint):
+    """The reference library (oracle/_ref, spqlios-fma) on this host's cores, one gate per thread;
+    the C oracle port (exact products) if the reference build is absent."""
+    import numpy as np
+    from tfhe_ref import RefLib
+    threads = os.cpu_count() or 1
+    ref = RefLib.load()
+    if ref is not None:
+        keys = ref.keygen(custom=None, seed=4242)
+        try:
+            per = 1
+            rng = np.random.default_rng(0)
+
+            def run(per_thread):
+                total = threads * per_thread
+                bits = rng.integers(0, 2, (2, total)).astype(np.int32)
+                a, b = keys.encrypt(bits[0]), keys.encrypt(bits[1])
+                out = np.zeros_like(a)
+                dt = keys.bench_gates(0, threads, per_thread, a, b, None, out)
+                got, _ = keys.decrypt(out)
+                return total, dt, int((got != 1 - (bits[0] & bits[1])).sum())
+
+            total, dt, _ = run(per)  # calibration
+            per = max(1, int(seconds / max(dt, 1e-3)))
+            total, dt, errors = run(per)
+            return {"value": total / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+                    "sample": f"{total} bootsNAND (default params) on {threads} threads, one gate per thread, "
+                              f"{dt:.1f} s, {errors} decryption errors"}
+        finally:
+            keys.free()
+    from tfhe_oracle import DEFAULT, Oracle
+    o = Oracle.get()
+    lk, tk, ksk, bsk = o.keygen(DEFAULT, seed=3)
+    rng = np.random.default_rng(0)
+    bits = rng.integers(0, 2, (2, 4))
+    a, b = o.encrypt_bits(lk, bits[0], seed=1), o.encrypt_bits(lk, bits[1], seed=2)
+    t0 = time.perf_counter()
+    o.gate(DEFAULT, bsk, ksk, 0, a, b)
+    dt = time.perf_counter() - t0
+    return {"value": 4 / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"4 bootsNAND through the C oracle (exact products), 1 thread, {dt:.1f} s"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    t0 = time.perf_counter()
+    vals = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(max(2.0, args.cpu_seconds / max(1, args.steps)), args.batch)
+        if i >= args.warmup:
+            vals.append(r["value"])
+            base = r
+    value = sum(vals) / len(vals)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "bootsNAND at the default 128-bit parameters on the host cores, "
+                                   "one gate per thread (tfhe v1.1 spqlios-fma)", "params": PARAMS},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"], "kind": base["kind"],
+                             "sample": base["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t0}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import tfhe_b200 as tb
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    p = tb.default_params()
+    sk, ck = tb.keygen(p, seed=1000 + rank)
+    ck.to_device(local_rank)
+    B = args.batch
+    rng = np.random.default_rng(rank)
+    bits = rng.integers(0, 2, (2, B))
+    ha, hb = sk.encrypt(bits[0], seed=11 + rank), sk.encrypt(bits[1], seed=12 + rank)
+    d_a = torch.from_numpy(ha).cuda()
+    d_b = torch.from_numpy(hb).cuda()
+    d_out = torch.zeros_like(d_a)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")  # 256 MiB > 126 MB L2
+    stream = torch.cuda.current_stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    L = tb.api.lib()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def measure(form):
+        precision = tb.SPLIT_FP32 if form == "split" else tb.FP64
+        for _ in range(args.warmup):
+            ck.gate_device(tb.api.NAND, d_a, d_b, None, d_out, B, precision=precision, stream=sptr)
+        torch.cuda.synchronize()
+        got, _ = sk.decrypt(d_out.cpu().numpy())
+        errors = int((got != 1 - (bits[0] & bits[1])).sum())
+        L.tfheb_profile(ck.h, 1)
+        L.tfheb_profile_read(ck.h, None, None, 1)
+        barrier()
+        torch.cuda.synchronize()
+        launches0 = tb.kernel_launches()
+        evs = []
+        for i in range(args.steps):
+            flush.fill_(i)  # evict the L2 between timed steps (outside the events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ck.gate_device(tb.api.NAND, d_a, d_b, None, d_out, B, precision=precision, stream=sptr)
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        barrier()
+        launches = tb.kernel_launches() - launches0
+        total_ms = sum(a.elapsed_time(b) for a, b in evs)
+        kms = (ctypes.c_double * 4)()
+        kn = (ctypes.c_int64 * 4)()
+        L.tfheb_profile_read(ck.h, kms, kn, 1)
+        L.tfheb_profile(ck.h, 0)
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return {"total_ms": float(t.item()), "errors": errors, "launches": launches,
+                "kernel_ms": [kms[i] / max(1, kn[i]) for i in range(4)], "kernel_n": [kn[i] for i in range(4)]}
+
+    # FMA throughput probe (roofline denominator at the current clocks)
+    peak = {}
+    for name, prec in (("fp32", tb.SPLIT_FP32), ("fp64", tb.FP64)):
+        v = ctypes.c_double()
+        L.tfheb_measure_fma_peak(local_rank, prec, ctypes.byref(v))
+        peak[name] = v.value
+
+    other = "fp64" if args.form == "split" else "split"
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    main_r = measure(args.form)
+    clk = clocks.stop()
+    other_r = measure(other)
+
+    gates = B * args.steps * world
+    value = gates / (main_r["total_ms"] / 1e3)
+    other_value = gates / (other_r["total_ms"] / 1e3)
+
+    # end to end through the public host API: pinned host inputs in, host outputs back, every step
+    pa = torch.from_numpy(ha).pin_memory()
+    pb = torch.from_numpy(hb).pin_memory()
+    po = torch.empty_like(pa).pin_memory()
+    precision = tb.SPLIT_FP32 if args.form == "split" else tb.FP64
+    L.tfheb_gate_batch(ck.h, tb.api.NAND, precision, B, ctypes.c_void_p(pa.data_ptr()),
+                       ctypes.c_void_p(pb.data_ptr()), None, ctypes.c_void_p(po.data_ptr()))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        st = L.tfheb_gate_batch(ck.h, tb.api.NAND, precision, B, ctypes.c_void_p(pa.data_ptr()),
+                                ctypes.c_void_p(pb.data_ptr()), None, ctypes.c_void_p(po.data_ptr()))
+        assert st == 0
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = B * args.e2e_steps * world / e2e_s
+    got, _ = sk.decrypt(po.numpy())
+    e2e_errors = int((got != 1 - (bits[0] & bits[1])).sum())
+
+    if rank == 0:
+        br_ms = main_r["kernel_ms"][1]
+        flops = FLOPS_PER_GATE[args.form] * B
+        achieved = flops / (br_ms / 1e3) / 1e12
+        pk = peak["fp32" if args.form == "split" else "fp64"]
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            traffic = json.load(open(tpath)).get(f"blind_rotate_{args.form}_bytes_per_launch")
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": main_r["total_ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.form == "split" else "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{B} independent bootsNAND per step (one batch), default 128-bit params, "
+                                   f"{'split-FP32' if args.form == 'split' else 'FP64'} external product",
+                       "params": PARAMS, "global_batch": B * world, "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB buffer written between timed steps (outside the events)"},
+            "errors": main_r["errors"],
+            "fp64" if args.form == "split" else "split": {
+                "value": other_value, "ms_per_step": other_r["total_ms"] / args.steps, "errors": other_r["errors"],
+                "kernel_ms": other_r["kernel_ms"]},
+            "kernel_ms": {"prologue": main_r["kernel_ms"][0], "blind_rotate": main_r["kernel_ms"][1],
+                          "extract": main_r["kernel_ms"][2], "keyswitch": main_r["kernel_ms"][3]},
+            "roofline": {"bound": "fp32" if args.form == "split" else "fp64", "kernel": "blind_rotate_kernel",
+                         "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
+                         "peak_source": "measured FMA-chain probe on this GPU (tfheb_measure_fma_peak)",
+                         "traffic": traffic,
+                         "algorithmic": f"{FLOPS_PER_GATE[args.form] / 1e6:.2f} MFLOP/gate x {B} gates per launch"},
+            "peaks_measured": peak,
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * B * (p.n + 1) * 4,
+                    "d2h_bytes_per_step": B * (p.n + 1) * 4, "errors": e2e_errors,
+                    "api": "tfheb_gate_batch (host buffers, pinned)"},
+            "gpu_launches": main_r["launches"],
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds, B)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -146,6 +146,20 @@ tfheb_status tfheb_keyswitch_device(tfheb_cloud_key *ck, int32_t count, const in
 /* Synchronise the key's stream and report any pending device error. */
 tfheb_status tfheb_synchronize(tfheb_cloud_key *ck);
 
+/* Per-kernel timing: when enabled, every kernel the key launches is bracketed by CUDA events on
+ * its stream.  read: ms[4] / launches[4] accumulated for prologue, blind rotation, extraction,
+ * keyswitch (reset != 0 clears the totals).  No reference counterpart (the reference has no
+ * instrumentation beyond clock() in its test programs). */
+tfheb_status tfheb_profile(tfheb_cloud_key *ck, int32_t enable);
+tfheb_status tfheb_profile_read(tfheb_cloud_key *ck, double *ms, int64_t *launches, int32_t reset);
+
+/* FP32 (precision 1) or FP64 (precision 0) fused multiply-add throughput of the device in TFLOP/s,
+ * measured by a dependent-chain probe kernel: the CUDA-core roofline denominator. */
+tfheb_status tfheb_measure_fma_peak(int32_t device, int32_t precision, double *tflops);
+
+/* Weight exponent S of the high limb the split-FP32 key uses by default for a parameter set. */
+int32_t tfheb_default_split_shift(const tfheb_params *p);
+
 /* Layout helpers (host only, no GPU): slot order of the FFT-domain key for ring degree N
  * (slot_freq[R*N/16]: frequency held by register r of thread t at index r*(N/16)+t). */
 tfheb_status tfheb_fft_slot_order(int32_t N, int32_t *slot_freq);

@@ -118,9 +118,38 @@ static tfheb_status ensure_device(CloudKey &ck, int precision) {
     return TFHEB_OK;
 }
 
+// Weight 2^S of the high limb in split mode.  The high-limb product must round to the exact
+// integer: its FP32 error is ~4 * 2^-24 * rms(product) with
+//   rms(product) = sqrt(N*(k+1)*l) * (2^Bgbit/sqrt12) * (2^(32-S)/sqrt12),
+// so S is the smallest shift keeping rms(product) <= 2^18 (error sigma <= 1/64 limb unit, >30 sigma
+// from a wrong rounding).  Default parameters give S = 24, the N=2048 set S = 26.
+int default_split_shift(const tfheb_params &p) {
+    const double terms = std::sqrt((double)p.N * (p.k + 1) * p.l);
+    const double digit_rms = std::ldexp(1.0, p.Bgbit) / std::sqrt(12.0);
+    for (int S = 16; S <= 30; S++) {
+        const double hi_rms = std::ldexp(1.0, 32 - S) / std::sqrt(12.0);
+        if (terms * digit_rms * hi_rms <= 262144.0) return S;
+    }
+    return 30;
+}
+
 static int default_gpb(const tfheb_params &p, int precision) {
     (void)precision;
     return p.N >= 2048 ? 1 : 2;
+}
+
+// Launch `fn` on stream s, bracketed by CUDA events when per-kernel profiling is on.
+template <typename Fn>
+static cudaError_t timed(CloudKey &ck, int which, cudaStream_t s, Fn &&fn) {
+    if (!ck.prof) return fn();
+    CloudKey::ProfRec r{which, nullptr, nullptr};
+    cudaEventCreate(&r.a);
+    cudaEventCreate(&r.b);
+    cudaEventRecord(r.a, s);
+    const cudaError_t e = fn();
+    cudaEventRecord(r.b, s);
+    ck.prof_pending.push_back(r);
+    return e;
 }
 
 // Device pipeline for `count` gates described by (bd, gd) already uploaded.
@@ -133,11 +162,15 @@ static tfheb_status run_pipeline(CloudKey &ck, int precision, int count, int boo
     if ((st = grow(ck.d_bara, ck.bara_cap, (size_t)boots * bs)) != TFHEB_OK) return st;
     if ((st = grow(ck.d_acc, ck.acc_cap, (size_t)boots * (p.k + 1) * p.N)) != TFHEB_OK) return st;
     if ((st = grow(ck.d_ksin, ck.ksin_cap, (size_t)count * kN1)) != TFHEB_OK) return st;
-    TFHEB_CUDA(launch_prologue(p, ck.d_bdesc, boots, d_a, d_b, d_c, ck.d_bara, bs, s));
-    TFHEB_CUDA(launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, boots, p.n,
-                                   modswitch_to_torus32(1, 8), nullptr, ck.d_acc, s, default_gpb(p, precision)));
-    TFHEB_CUDA(launch_extract(p, ck.d_gdesc, count, ck.d_acc, ck.d_ksin, kN1, s));
-    TFHEB_CUDA(launch_keyswitch(p, ck.d_ksk, ck.ks_stride, count, ck.d_ksin, kN1, d_out, s));
+    TFHEB_CUDA(timed(ck, 0, s, [&] { return launch_prologue(p, ck.d_bdesc, boots, d_a, d_b, d_c, ck.d_bara, bs, s); }));
+    TFHEB_CUDA(timed(ck, 1, s, [&] {
+        return launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, boots, p.n,
+                                   modswitch_to_torus32(1, 8), nullptr, ck.d_acc, s, default_gpb(p, precision));
+    }));
+    TFHEB_CUDA(timed(ck, 2, s, [&] { return launch_extract(p, ck.d_gdesc, count, ck.d_acc, ck.d_ksin, kN1, s); }));
+    TFHEB_CUDA(timed(ck, 3, s, [&] {
+        return launch_keyswitch(p, ck.d_ksk, ck.ks_stride, count, ck.d_ksin, kN1, d_out, s);
+    }));
     g_launches += 4;
     ck.launches += 4;
     return TFHEB_OK;
@@ -302,7 +335,7 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32
         set_error("no compiled blind-rotation kernel for this parameter set");
         return TFHEB_ERR_UNSUPPORTED;
     }
-    if (split_shift == 0) split_shift = 24;
+    if (split_shift == 0) split_shift = default_split_shift(ck.p);
     if (split_shift < 8 || split_shift > 30) return TFHEB_ERR_INVALID;
     TFHEB_CUDA(cudaSetDevice(device));
     ck.device = device;
@@ -510,6 +543,47 @@ tfheb_status tfheb_synchronize(tfheb_cloud_key *c) {
     TFHEB_CUDA(cudaGetLastError());
     return TFHEB_OK;
 }
+
+tfheb_status tfheb_profile(tfheb_cloud_key *c, int32_t enable) {
+    if (!c) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->ck.prof = enable != 0;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_profile_read(tfheb_cloud_key *c, double *ms, int64_t *launches, int32_t reset) {
+    if (!c) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    for (auto &r : ck.prof_pending) {
+        float t = 0;
+        cudaEventSynchronize(r.b);
+        cudaEventElapsedTime(&t, r.a, r.b);
+        ck.prof_ms[r.which] += t;
+        ck.prof_n[r.which] += 1;
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    ck.prof_pending.clear();
+    for (int i = 0; i < 4; i++) {
+        if (ms) ms[i] = ck.prof_ms[i];
+        if (launches) launches[i] = ck.prof_n[i];
+        if (reset) {
+            ck.prof_ms[i] = 0;
+            ck.prof_n[i] = 0;
+        }
+    }
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_measure_fma_peak(int32_t device, int32_t precision, double *tflops) {
+    if (!tflops || (precision != TFHEB_FP64 && precision != TFHEB_SPLIT_FP32)) return TFHEB_ERR_INVALID;
+    TFHEB_CUDA(cudaSetDevice(device));
+    TFHEB_CUDA(measure_fma_peak(precision, tflops));
+    return TFHEB_OK;
+}
+
+int32_t tfheb_default_split_shift(const tfheb_params *p) { return p ? default_split_shift(*p) : 0; }
 
 tfheb_status tfheb_fft_slot_order(int32_t N, int32_t *slot_freq) {
     std::vector<int32_t> sf;

@@ -65,6 +65,15 @@ struct CloudKey {
     int cached_gate = -1, cached_count = -1;
     int32_t *d_err = nullptr;       // device error word
     int launches = 0;               // kernels launched (for the bench's launch count)
+    // optional per-kernel timing with CUDA events on the launching stream
+    bool prof = false;
+    struct ProfRec {
+        int which;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfRec> prof_pending;
+    double prof_ms[4] = {0, 0, 0, 0};  // prologue, blind rotation, extraction, keyswitch
+    int64_t prof_n[4] = {0, 0, 0, 0};
 };
 
 struct SecretKey {
@@ -98,6 +107,9 @@ cudaError_t launch_keyswitch(const tfheb_params &p, const int32_t *d_ksk, int ks
                              const int32_t *in, int in_stride, int32_t *out, cudaStream_t s);
 int blind_rotate_supported(const tfheb_params &p);
 cudaError_t launch_negate(const int32_t *in, int32_t *out, size_t count, cudaStream_t s);
+
+int default_split_shift(const tfheb_params &p);
+cudaError_t measure_fma_peak(int precision, double *tflops);
 
 // ---- errors ---------------------------------------------------------------------------------
 void set_error(const std::string &msg);

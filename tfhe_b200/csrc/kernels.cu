@@ -443,4 +443,53 @@ cudaError_t launch_keyswitch(const tfheb_params &p, const int32_t *d_ksk, int ks
     return cudaGetLastError();
 }
 
+// ============================================================================================
+// FMA throughput probe: the FP32 / FP64 CUDA-core roofline denominator of the blind rotation,
+// measured on the running GPU at its current clocks (8 independent FMA chains per thread).
+// ============================================================================================
+
+template <typename T>
+__global__ void fma_peak_kernel(T *out, int iters, T a, T b) {
+    T x0 = T(threadIdx.x), x1 = x0 + T(1), x2 = x0 + T(2), x3 = x0 + T(3);
+    T x4 = x0 + T(4), x5 = x0 + T(5), x6 = x0 + T(6), x7 = x0 + T(7);
+    for (int i = 0; i < iters; i++) {
+        x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+        x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+    const T s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+    if (s == T(-1234.5)) out[0] = s;  // keeps the chains live
+}
+
+cudaError_t measure_fma_peak(int precision, double *tflops) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    void *out = nullptr;
+    cudaError_t e = cudaMalloc(&out, 16);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(e0);
+        if (precision == TFHEB_FP64)
+            fma_peak_kernel<double><<<blocks, threads>>>((double *)out, iters, 0.999999, 1e-7);
+        else
+            fma_peak_kernel<float><<<blocks, threads>>>((float *)out, iters, 0.9999f, 1e-7f);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) best = std::min(best, ms);
+    }
+    e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (best * 1e-3) / 1e12;
+    return e;
+}
+
 }  // namespace tfheb
