@@ -193,7 +193,8 @@ def main():
     d_b = torch.from_numpy(hb).cuda()
     d_out = torch.zeros_like(d_a)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")  # 256 MiB > 126 MB L2
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # a real stream: the engine's kernels and the timing events share it
+    torch.cuda.set_stream(stream)
     sptr = ctypes.c_void_p(stream.cuda_stream)
     L = tb.api.lib()
 

@@ -131,8 +131,10 @@ def test_cmux_step_split_fp32_error_bound(oracle, request, ring):
     err = cmux_errors(oracle, p, ck, bsk, tb.SPLIT_FP32, count=4)
     rms = float(np.sqrt((err.astype(np.float64) ** 2).mean()))
     print(f"split-FP32 CMUX error vs exact (N={p.N}): max {np.abs(err).max()} units, rms {rms:.1f} units")
-    assert np.abs(err).max() < 2**17
-    assert rms < 2**14
+    # the low limb carries 2^S with S = 24 (N=1024) / 26 (N=2048): its FP32 error scales with 2^S
+    scale = 1 if p.N == 1024 else 4
+    assert np.abs(err).max() < scale * 2**17
+    assert rms < scale * 2**14
 
 
 def test_blind_rotate_many_steps_fp64_matches_oracle(oracle, default_keys):
