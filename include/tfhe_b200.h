@@ -103,7 +103,8 @@ tfheb_status tfheb_decrypt(const tfheb_secret_key *sk, const int32_t *cts, int32
 /* Moves the cloud key to a GPU: FFT-domain bootstrapping key in the requested precisions
  * (bit 0 = FP64, bit 1 = split FP32), keyswitching key, twiddle tables.  The host-side FP64
  * transform replaces init_LweBootstrappingKeyFFT (lwe-bootstrapping-functions-fft.cpp:23-52).
- * split_shift: weight 2^split_shift of the high limb in split mode (0 = default 24). */
+ * split_shift: weight 2^split_shift of the high limb in split mode (0 = the parameter-dependent
+ * default of tfheb_default_split_shift). */
 tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *ck, int32_t device, int32_t precision_mask,
                                        int32_t split_shift);
 
@@ -143,8 +144,18 @@ tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *ck, int32_t precision, i
 tfheb_status tfheb_keyswitch_device(tfheb_cloud_key *ck, int32_t count, const int32_t *d_in, int32_t *d_out,
                                     void *stream);
 
-/* Synchronise the key's stream and report any pending device error. */
+/* Synchronise the key's stream and report any pending device error (TFHEB_ERR_TIMEOUT when a
+ * bounded device-side wait of a kernel ran out). */
 tfheb_status tfheb_synchronize(tfheb_cloud_key *ck);
+
+/* Limit of every device-side wait of the key's kernels (default 1 s).  The reference has no
+ * device waits; this is the failure-detection knob of the GPU engine. */
+tfheb_status tfheb_set_wait_timeout(tfheb_cloud_key *ck, uint64_t timeout_ns);
+
+/* Failure-detection test hook: when set, the blind rotation's key-streaming warp issues no copies,
+ * so every consumer wait runs out after the timeout and the launch reports TFHEB_ERR_TIMEOUT with
+ * the context still usable.  No reference counterpart. */
+tfheb_status tfheb_test_stall_key_stream(tfheb_cloud_key *ck, int32_t stall);
 
 /* Per-kernel timing: when enabled, every kernel the key launches is bracketed by CUDA events on
  * its stream.  read: ms[4] / launches[4] accumulated for prologue, blind rotation, extraction,

@@ -25,7 +25,12 @@ FP64, SPLIT_FP32 = 0, 1
 
 
 class TfhebError(RuntimeError):
-    pass
+    def __init__(self, msg, status=None):
+        super().__init__(msg)
+        self.status = status
+
+
+TIMEOUT = 5
 
 
 class Params(ctypes.Structure):
@@ -64,6 +69,8 @@ def lib():
         L.tfheb_blind_rotate_device.argtypes = [_V, _I32, _I32, _I32, _V, _V, _V]
         L.tfheb_keyswitch_device.argtypes = [_V, _I32, _V, _V, _V]
         L.tfheb_synchronize.argtypes = [_V]
+        L.tfheb_set_wait_timeout.argtypes = [_V, ctypes.c_uint64]
+        L.tfheb_test_stall_key_stream.argtypes = [_V, _I32]
         L.tfheb_fft_slot_order.argtypes = [_I32, _V]
         _lib = L
     return _lib
@@ -72,7 +79,7 @@ def lib():
 def _check(status, what):
     if status != 0:
         msg = lib().tfheb_last_error().decode(errors="replace")
-        raise TfhebError(f"{what} failed with status {status}: {msg}")
+        raise TfhebError(f"{what} failed with status {status}: {msg}", status)
 
 
 def _p(a):
@@ -203,6 +210,12 @@ class CloudKey:
 
     def keyswitch_device(self, d_in, d_out, count, stream=None):
         _check(lib().tfheb_keyswitch_device(self.h, count, _p(d_in), _p(d_out), stream), "tfheb_keyswitch_device")
+
+    def set_wait_timeout(self, seconds):
+        _check(lib().tfheb_set_wait_timeout(self.h, ctypes.c_uint64(int(seconds * 1e9))), "tfheb_set_wait_timeout")
+
+    def test_stall_key_stream(self, stall=True):
+        _check(lib().tfheb_test_stall_key_stream(self.h, 1 if stall else 0), "tfheb_test_stall_key_stream")
 
     def synchronize(self):
         _check(lib().tfheb_synchronize(self.h), "tfheb_synchronize")

@@ -1,0 +1,413 @@
+// blind_rotate.cu -- persistent blind rotation on sm_100a (tfhe_blindRotate_FFT,
+// lwe-bootstrapping-functions-fft.cpp:88-112, with tfhe_MuxRotate_FFT :67-76 and the external
+// product tGswFFTExternMulToTLwe, tgsw-fft-operations.cpp:89-114).
+//
+// One CTA = G "teams" (one bootstrap each, N/16 threads per team) + one producer warp.
+//   * Each team keeps its accumulator TLWE (k+1 polynomials of N Torus32) in shared memory for all
+//     n CMUX steps.  Per step: rotation (X^a - 1)*acc, gadget decomposition, a forward negacyclic FFT
+//     per digit polynomial (fft.cuh), multiply-accumulate against the bootstrapping-key row in the
+//     FFT domain, inverse FFTs, rounding back to Torus32 and accumulation.
+//   * The bootstrapping key is streamed once per CTA: the producer warp copies each key row
+//     ((k+1) x N/2 slots x 16 bytes = 16 KB at N=1024) with a bulk asynchronous copy (TMA engine,
+//     cp.async.bulk, no multicast) into a D-stage shared-memory ring guarded by mbarriers; all G teams
+//     read the same stage.  L2->SM key traffic is therefore 62 MB per G bootstraps instead of per
+//     bootstrap.
+//   * Every mbarrier wait is bounded (%globaltimer).  On expiry the CTA raises a shared abort flag,
+//     every later wait returns at once (the FFT barriers stay uniform, so nothing hangs), the
+//     producer drains its in-flight copies, and the host reads TFHEB_ERR_TIMEOUT from the error word.
+//
+// Precision forms:
+//   FP64  (SPLIT=false): key row slot = double2 B_k / M; products rounded with the 1.5*2^52 addition
+//          (exact round-to-nearest for |x| < 2^51), reduced mod 2^32.
+//   split (SPLIT=true):  key coefficient c = hi * 2^S + lo (S from default_split_shift); slot =
+//          float4 (hi, lo) spectra / M; both limb products are rounded exactly and recombined as
+//          hi * 2^S + lo mod 2^32.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft.cuh"
+#include "internal.h"
+
+namespace tfheb {
+
+// ---- PTX helpers ----------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_timer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// bulk global -> shared copy completing on an mbarrier (size multiple of 16, 16-byte aligned ends)
+__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// Bounded wait: true when the phase completed, false on timeout or when the CTA already aborted.
+__device__ __forceinline__ bool wait_bounded(uint32_t bar, uint32_t parity, volatile int32_t *abort_flag,
+                                             uint64_t timeout_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_timer_ns();
+    for (;;) {
+        if (*abort_flag) return false;
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_timer_ns() - t0 > timeout_ns) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+}
+
+// ---- exact conversions without the conversion (XU) pipe ------------------------------------
+
+// small integer v (|v| < 2^22) -> float, via the 1.5*2^23 bias
+__device__ __forceinline__ float biased_to_float(uint32_t biased_bits_minus_magic, float bias) {
+    return __int_as_float(0x4B400000 + (int32_t)biased_bits_minus_magic) - bias;
+}
+// round-to-nearest of a float with |v| < 2^44, reduced mod 2^32 (FMA/ALU ops only)
+__device__ __forceinline__ uint32_t round_f32_mod32(float v) {
+    const float magic = 12582912.0f;  // 1.5 * 2^23
+    const float m1 = fmaf(v, 0x1.0p-22f, magic);
+    const uint32_t th = (uint32_t)(__float_as_int(m1) - 0x4B400000);
+    const float r = fmaf(-(m1 - magic), 4194304.0f, v);  // exact: |r| <= 2^21
+    const uint32_t tl = (uint32_t)(__float_as_int(r + magic) - 0x4B400000);
+    return (th << 22) + tl;
+}
+// round-to-nearest of a double with |v| < 2^51, reduced mod 2^32
+__device__ __forceinline__ uint32_t round_f64_mod32(double v) {
+    return (uint32_t)__double2loint(v + 6755399441055744.0);  // 1.5 * 2^52
+}
+
+template <typename T>
+struct DigitConv;
+template <>
+struct DigitConv<float> {
+    // value d - halfBg of a raw digit d in [0, Bg)
+    __device__ __forceinline__ static float conv(uint32_t d, float bias) { return biased_to_float(d, bias); }
+    __host__ __device__ static constexpr float base() { return 12582912.0f; }
+};
+template <>
+struct DigitConv<double> {
+    __device__ __forceinline__ static double conv(uint32_t d, double bias) {
+        return __hiloint2double(0x43380000, (int)d) - bias;
+    }
+    __host__ __device__ static constexpr double base() { return 6755399441055744.0; }
+};
+
+// ---- shared-memory layout ---------------------------------------------------------------------
+
+template <typename T, int N, int K, int G, int D>
+struct BrLayout {
+    static constexpr int M = N / 2, NT = M / kR, KP1 = K + 1;
+    static constexpr int TW = tw_offset<M>(FftPlan<M>::NS);
+    static constexpr uint32_t chunk = (uint32_t)KP1 * M * 16;  // one key row (step, p): all v, all slots
+    static constexpr size_t bars = 0;                           // full[D], empty[D], abort flag
+    static constexpr size_t ring = 128;
+    static constexpr size_t tables = ring + (size_t)D * chunk;
+    static constexpr size_t tables_bytes = ((sizeof(cplx<T>) * (TW + kR * NT)) + 15) / 16 * 16;
+    static constexpr size_t teams = tables + tables_bytes;
+    static constexpr size_t team_acc = 4 * (size_t)KP1 * N;
+    static constexpr size_t team_buf = 2 * sizeof(T) * M;
+    __host__ __device__ static size_t team_bytes(int nsteps) {
+        return team_acc + team_buf + 16 * (((size_t)nsteps + 4 + 3) / 4);
+    }
+    __host__ __device__ static size_t bytes(int nsteps) { return teams + G * team_bytes(nsteps); }
+    static_assert(2 * D * 8 + 4 <= 128, "barrier block");
+};
+
+struct BrArgs {
+    const int32_t *bara;
+    int bara_stride;
+    const uint8_t *bsk;
+    const void *tables;
+    const int32_t *acc_in;
+    int32_t *acc_out;
+    int boots, nsteps;
+    int32_t mu;
+    int Bgbit;
+    int split_shift;
+    int32_t *err;
+    uint64_t timeout_ns;
+    int stall_producer;
+};
+
+// (X^a - 1) * acc, coefficient j (toruspolynomial-functions.cpp:117-136), 0 <= a < 2N
+template <int N>
+__device__ __forceinline__ uint32_t rot_minus_one(const uint32_t *poly, int j, int a) {
+    const int src = j - a;
+    uint32_t v;
+    if (src >= 0) v = poly[src];
+    else if (src >= -N) v = 0u - poly[src + N];
+    else v = poly[src + 2 * N];
+    return v - poly[j];
+}
+
+template <typename T, int N, int K, int L, bool SPLIT, int G, int D>
+__global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const BrArgs args) {
+    using Lay = BrLayout<T, N, K, G, D>;
+    constexpr int M = N / 2, NT = M / kR, KP1 = K + 1, KPL = KP1 * L;
+    using F = TeamFft<T, M, kR>;
+    extern __shared__ __align__(128) unsigned char smem[];
+
+    const int tid = threadIdx.x;
+    const int consumers = G * NT;
+    const int active_teams = min(G, args.boots - (int)blockIdx.x * G);
+    const uint32_t bar0 = smem_addr(smem + Lay::bars);
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (D + s); };
+    volatile int32_t *abort_flag = reinterpret_cast<volatile int32_t *>(smem + Lay::bars + 16 * D);
+    const uint32_t ring = smem_addr(smem + Lay::ring);
+
+    if (tid == 0) {
+        for (int s = 0; s < D; s++) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), (uint32_t)(active_teams * NT));
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    cplx<T> *s_tab = reinterpret_cast<cplx<T> *>(smem + Lay::tables);
+    const cplx<T> *g_tab = reinterpret_cast<const cplx<T> *>(args.tables);
+    for (int i = tid; i < Lay::TW + kR * NT; i += blockDim.x) s_tab[i] = g_tab[i];
+    __syncthreads();
+
+    const int total_chunks = args.nsteps * KPL;
+
+    // ---------------- producer warp: stream the key rows ----------------
+    if (tid >= consumers) {
+        if (tid == consumers) {
+            int issued = 0;
+            if (!args.stall_producer) {
+                for (int c = 0; c < total_chunks; c++) {
+                    const int s = c % D;
+                    if (c >= D && !wait_bounded(empty_bar(s), ((c / D) - 1) & 1, abort_flag, args.timeout_ns)) break;
+                    mbar_arrive_expect_tx(full_bar(s), Lay::chunk);
+                    bulk_copy_g2s(ring + (uint32_t)s * Lay::chunk, args.bsk + (size_t)c * Lay::chunk, Lay::chunk,
+                                  full_bar(s));
+                    issued = c + 1;
+                }
+            }
+            // drain the copies still in flight before the CTA may exit (each wait bounded)
+            volatile int32_t no_abort = 0;
+            for (int c = (issued > D ? issued - D : 0); c < issued; c++)
+                wait_bounded(full_bar(c % D), (c / D) & 1, &no_abort, args.timeout_ns);
+            if (*abort_flag) atomicOr(args.err, 1);
+        }
+        return;
+    }
+
+    // ---------------- consumer teams ----------------
+    const int team = tid / NT;
+    const int t = tid - team * NT;
+    if (team >= active_teams) return;  // not counted in the empty barriers; no CTA barrier follows
+    const int boot = blockIdx.x * G + team;
+    const int bar_id = 1 + team;
+
+    unsigned char *tb = smem + Lay::teams + (size_t)team * Lay::team_bytes(args.nsteps);
+    uint32_t *s_acc = reinterpret_cast<uint32_t *>(tb);
+    T *buf_re = reinterpret_cast<T *>(tb + Lay::team_acc);
+    T *buf_im = buf_re + M;
+    int32_t *s_bara = reinterpret_cast<int32_t *>(tb + Lay::team_acc + Lay::team_buf);
+    const cplx<T> *s_tw = s_tab;
+    const cplx<T> *s_twist = s_tab + Lay::TW;
+
+    const int32_t *my_bara = args.bara + (size_t)boot * args.bara_stride;
+    for (int i = t; i < args.nsteps; i += NT) s_bara[i] = my_bara[i];
+    if (args.acc_in) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(args.acc_in) + (size_t)boot * KP1 * N;
+        for (int i = t; i < KP1 * N; i += NT) s_acc[i] = src[i];
+    } else {
+        // acc = (0, X^{2N-barb} * [mu,...,mu])  (lwe-bootstrapping-functions-fft.cpp:142-145)
+        const int e = 2 * N - my_bara[args.nsteps];
+        for (int i = t; i < K * N; i += NT) s_acc[i] = 0u;
+        for (int j = t; j < N; j += NT) {
+            int src = j - e;
+            uint32_t neg = 0;
+            while (src < 0) {
+                src += N;
+                neg ^= 1u;
+            }
+            s_acc[K * N + j] = neg ? 0u - (uint32_t)args.mu : (uint32_t)args.mu;
+        }
+    }
+    team_sync(bar_id, NT);
+
+    // gadget constants (tgsw.cpp:7-29)
+    const int Bgbit = args.Bgbit;
+    uint32_t offset = 0;
+#pragma unroll
+    for (int q = 0; q < L; q++) offset += 1u << (32 - (q + 1) * Bgbit);
+    offset *= 1u << (Bgbit - 1);
+    const uint32_t maskBg = (1u << Bgbit) - 1u;
+    const T digit_bias = DigitConv<T>::base() + T(1 << (Bgbit - 1));
+
+    int c = 0;  // key-row (chunk) counter, same sequence as the producer
+    for (int step = 0; step < args.nsteps; step++) {
+        const int ai = s_bara[step] & (2 * N - 1);
+        cplx<T> acc_hi[KP1][kR];
+        cplx<T> acc_lo[SPLIT ? KP1 : 1][kR];
+#pragma unroll
+        for (int v = 0; v < KP1; v++)
+#pragma unroll
+            for (int r = 0; r < kR; r++) {
+                acc_hi[v][r] = {T(0), T(0)};
+                if (SPLIT) acc_lo[SPLIT ? v : 0][r] = {T(0), T(0)};
+            }
+
+#pragma unroll 1
+        for (int u = 0; u < KP1; u++) {
+            const uint32_t *poly = s_acc + u * N;
+            uint32_t x0[kR], x1[kR];
+#pragma unroll
+            for (int r = 0; r < kR; r++) {
+                const int j = t + NT * r;
+                x0[r] = rot_minus_one<N>(poly, j, ai) + offset;
+                x1[r] = rot_minus_one<N>(poly, j + M, ai) + offset;
+            }
+#pragma unroll 1
+            for (int q = 0; q < L; q++, c++) {
+                const int shift = 32 - (q + 1) * Bgbit;
+                cplx<T> z[kR];
+#pragma unroll
+                for (int r = 0; r < kR; r++) {
+                    const T d0 = DigitConv<T>::conv((x0[r] >> shift) & maskBg, digit_bias);
+                    const T d1 = DigitConv<T>::conv((x1[r] >> shift) & maskBg, digit_bias);
+                    z[r] = cmul(cplx<T>{d0, -d1}, s_twist[r * NT + t]);  // (a_j - i a_{j+M}) e^{-i pi j/N}
+                }
+                F::forward(z, buf_re, buf_im, s_tw, t, bar_id);
+
+                const int s = c % D;
+                wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns);
+                const unsigned char *stage = smem + Lay::ring + (size_t)s * Lay::chunk;
+#pragma unroll
+                for (int v = 0; v < KP1; v++)
+#pragma unroll
+                    for (int r = 0; r < kR; r++) {
+                        const size_t off = ((size_t)(v * kR + r) * NT + t) * 16;
+                        if constexpr (SPLIT) {
+                            const float4 b = *reinterpret_cast<const float4 *>(stage + off);
+                            cmac(acc_hi[v][r], z[r], cplx<T>{b.x, b.y});
+                            cmac(acc_lo[SPLIT ? v : 0][r], z[r], cplx<T>{b.z, b.w});
+                        } else {
+                            const double2 b = *reinterpret_cast<const double2 *>(stage + off);
+                            cmac(acc_hi[v][r], z[r], cplx<T>{(T)b.x, (T)b.y});
+                        }
+                    }
+                mbar_arrive(empty_bar(s));
+            }
+        }
+
+        // inverse transforms, exact rounding, accumulate (the key was pre-scaled by 1/M)
+#pragma unroll
+        for (int v = 0; v < KP1; v++) {
+            uint32_t c0[kR], c1[kR];
+            {
+                cplx<T> z[kR];
+#pragma unroll
+                for (int r = 0; r < kR; r++) z[r] = acc_hi[v][r];
+                F::inverse(z, buf_re, buf_im, s_tw, t, bar_id);
+#pragma unroll
+                for (int r = 0; r < kR; r++) {
+                    const cplx<T> w = cmulconj(z[r], s_twist[r * NT + t]);  // (c_j - i c_{j+M})
+                    if constexpr (SPLIT) {
+                        c0[r] = round_f32_mod32(w.re) << args.split_shift;
+                        c1[r] = round_f32_mod32(-w.im) << args.split_shift;
+                    } else {
+                        c0[r] = round_f64_mod32(w.re);
+                        c1[r] = round_f64_mod32(-w.im);
+                    }
+                }
+            }
+            if constexpr (SPLIT) {
+                cplx<T> z[kR];
+#pragma unroll
+                for (int r = 0; r < kR; r++) z[r] = acc_lo[SPLIT ? v : 0][r];
+                F::inverse(z, buf_re, buf_im, s_tw, t, bar_id);
+#pragma unroll
+                for (int r = 0; r < kR; r++) {
+                    const cplx<T> w = cmulconj(z[r], s_twist[r * NT + t]);
+                    c0[r] += (uint32_t)__float2ll_rn(w.re);
+                    c1[r] += (uint32_t)__float2ll_rn(-w.im);
+                }
+            }
+            uint32_t *poly = s_acc + v * N;
+#pragma unroll
+            for (int r = 0; r < kR; r++) {
+                const int j = t + NT * r;
+                poly[j] += c0[r];
+                poly[j + M] += c1[r];
+            }
+        }
+        team_sync(bar_id, NT);
+    }
+
+    uint32_t *dst = reinterpret_cast<uint32_t *>(args.acc_out) + (size_t)boot * KP1 * N;
+    for (int i = t; i < KP1 * N; i += NT) dst[i] = s_acc[i];
+}
+
+// ---- launch -------------------------------------------------------------------------------------
+
+template <typename T, int N, bool SPLIT, int G, int D>
+static cudaError_t launch_g(const BrArgs &a, cudaStream_t s) {
+    using Lay = BrLayout<T, N, 1, G, D>;
+    const size_t smem = Lay::bytes(a.nsteps);
+    auto kern = blind_rotate_kernel<T, N, 1, 3, SPLIT, G, D>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.boots + G - 1) / G;
+    kern<<<grid, G * (N / 16) + 32, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+int blind_rotate_supported(const tfheb_params &p) {
+    if (p.k != 1 || p.l != 3) return 0;
+    return p.N == 512 || p.N == 1024 || p.N == 2048;
+}
+
+// bootstraps per CTA for (N, precision); each variant's shared memory stays within 227 KB
+int br_teams_per_cta(int N, int precision) {
+    if (N == 2048) return precision == TFHEB_FP64 ? 2 : 3;
+    if (N == 1024) return precision == TFHEB_FP64 ? 4 : 7;
+    return 8;
+}
+
+cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const DeviceBsk &bsk, const int32_t *bara,
+                                int bara_stride, int boots, int nsteps, int32_t mu, const int32_t *acc_in,
+                                int32_t *acc_out, cudaStream_t s, int32_t *d_err, int stall_producer,
+                                uint64_t timeout_ns) {
+    if (boots <= 0) return cudaSuccess;
+    BrArgs a{bara, bara_stride, reinterpret_cast<const uint8_t *>(bsk.bsk), bsk.tables, acc_in, acc_out, boots,
+             nsteps, mu, p.Bgbit, bsk.split_shift, d_err, timeout_ns, stall_producer};
+    const bool sp = precision == TFHEB_SPLIT_FP32;
+    switch (p.N) {
+        case 512: return sp ? launch_g<float, 512, true, 8, 4>(a, s) : launch_g<double, 512, false, 8, 4>(a, s);
+        case 1024: return sp ? launch_g<float, 1024, true, 7, 4>(a, s) : launch_g<double, 1024, false, 4, 4>(a, s);
+        case 2048: return sp ? launch_g<float, 2048, true, 3, 3>(a, s) : launch_g<double, 2048, false, 2, 3>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace tfheb

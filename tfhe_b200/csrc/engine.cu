@@ -133,10 +133,6 @@ int default_split_shift(const tfheb_params &p) {
     return 30;
 }
 
-static int default_gpb(const tfheb_params &p, int precision) {
-    (void)precision;
-    return p.N >= 2048 ? 1 : 2;
-}
 
 // Launch `fn` on stream s, bracketed by CUDA events when per-kernel profiling is on.
 template <typename Fn>
@@ -165,7 +161,8 @@ static tfheb_status run_pipeline(CloudKey &ck, int precision, int count, int boo
     TFHEB_CUDA(timed(ck, 0, s, [&] { return launch_prologue(p, ck.d_bdesc, boots, d_a, d_b, d_c, ck.d_bara, bs, s); }));
     TFHEB_CUDA(timed(ck, 1, s, [&] {
         return launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, boots, p.n,
-                                   modswitch_to_torus32(1, 8), nullptr, ck.d_acc, s, default_gpb(p, precision));
+                                   modswitch_to_torus32(1, 8), nullptr, ck.d_acc, s, ck.d_err, ck.stall_producer,
+                                   ck.wait_timeout_ns);
     }));
     TFHEB_CUDA(timed(ck, 2, s, [&] { return launch_extract(p, ck.d_gdesc, count, ck.d_acc, ck.d_ksin, kN1, s); }));
     TFHEB_CUDA(timed(ck, 3, s, [&] {
@@ -173,6 +170,18 @@ static tfheb_status run_pipeline(CloudKey &ck, int precision, int count, int boo
     }));
     g_launches += 4;
     ck.launches += 4;
+    return TFHEB_OK;
+}
+
+// Reads and clears the key's device error word (after the stream has been synchronised).
+static tfheb_status check_device_error(CloudKey &ck) {
+    int32_t err = 0;
+    TFHEB_CUDA(cudaMemcpy(&err, ck.d_err, sizeof(err), cudaMemcpyDeviceToHost));
+    if (err) {
+        TFHEB_CUDA(cudaMemset(ck.d_err, 0, sizeof(err)));
+        set_error("a bounded device-side wait expired (key stream stalled); results of that launch are invalid");
+        return TFHEB_ERR_TIMEOUT;
+    }
     return TFHEB_OK;
 }
 
@@ -340,6 +349,10 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32
     TFHEB_CUDA(cudaSetDevice(device));
     ck.device = device;
     if (!ck.stream) TFHEB_CUDA(cudaStreamCreateWithFlags(&ck.stream, cudaStreamNonBlocking));
+    if (!ck.d_err) {
+        TFHEB_CUDA(cudaMalloc((void **)&ck.d_err, sizeof(int32_t)));
+        TFHEB_CUDA(cudaMemset(ck.d_err, 0, sizeof(int32_t)));
+    }
     const tfheb_params &p = ck.p;
     // keyswitching key, rows padded to a multiple of 4 int32 (16-byte aligned vector loads)
     if (!ck.d_ksk) {
@@ -443,7 +456,7 @@ tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precisio
     std::lock_guard<std::mutex> lock(c->mu);
     TFHEB_CUDA(cudaMemcpyAsync(out, dio + 3 * sz, sz * 4, cudaMemcpyDeviceToHost, ck.stream));
     TFHEB_CUDA(cudaStreamSynchronize(ck.stream));
-    return TFHEB_OK;
+    return check_device_error(ck);
 }
 
 tfheb_status tfheb_gate_batch_mixed_device(tfheb_cloud_key *c, int32_t precision, int32_t count, const int32_t *gates,
@@ -479,7 +492,7 @@ tfheb_status tfheb_bootstrap_woks_device(tfheb_cloud_key *c, int32_t precision, 
     if ((st = grow(ck.d_acc, ck.acc_cap, (size_t)count * (p.k + 1) * p.N)) != TFHEB_OK) return st;
     TFHEB_CUDA(launch_prologue(p, ck.d_bdesc, count, d_in, d_in, d_in, ck.d_bara, bs, s));
     TFHEB_CUDA(launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, count, p.n, mu, nullptr,
-                                   ck.d_acc, s, default_gpb(p, precision)));
+                                   ck.d_acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns));
     TFHEB_CUDA(launch_extract(p, ck.d_gdesc, count, ck.d_acc, d_out, p.k * p.N + 1, s));
     g_launches += 3;
     return TFHEB_OK;
@@ -515,7 +528,7 @@ tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *c, int32_t precision, in
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
     // in place: acc_in == acc_out is safe (each team reads its row fully before writing it back)
     TFHEB_CUDA(launch_blind_rotate(ck.p, precision, ck.dbsk[precision], d_bara, nsteps, count, nsteps, 0, d_acc,
-                                   d_acc, s, default_gpb(ck.p, precision)));
+                                   d_acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns));
     g_launches += 1;
     return TFHEB_OK;
 }
@@ -540,7 +553,22 @@ tfheb_status tfheb_synchronize(tfheb_cloud_key *c) {
     if (ck.device < 0) return TFHEB_OK;
     TFHEB_CUDA(cudaSetDevice(ck.device));
     TFHEB_CUDA(cudaStreamSynchronize(ck.stream));
+    TFHEB_CUDA(cudaDeviceSynchronize());
     TFHEB_CUDA(cudaGetLastError());
+    return check_device_error(ck);
+}
+
+tfheb_status tfheb_set_wait_timeout(tfheb_cloud_key *c, uint64_t timeout_ns) {
+    if (!c || timeout_ns == 0) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->ck.wait_timeout_ns = timeout_ns;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_test_stall_key_stream(tfheb_cloud_key *c, int32_t stall) {
+    if (!c) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->ck.stall_producer = stall != 0;
     return TFHEB_OK;
 }
 

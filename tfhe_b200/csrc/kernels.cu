@@ -2,11 +2,7 @@
 //
 //   prologue_kernel      gate linear combination + modulus switch to Z_2N   (boot-gates.cpp:34-370,
 //                        lwe-bootstrapping-functions-fft.cpp:184-188, numeric-functions.cpp:59-65)
-//   blind_rotate_kernel  persistent blind rotation: accumulator resident in shared memory for all
-//                        n CMUX steps; per step rotation, gadget decomposition, negacyclic FFT,
-//                        FFT-domain MAC against the bootstrapping key, inverse FFT, accumulate
-//                        (lwe-bootstrapping-functions-fft.cpp:67-156, tgsw-fft-operations.cpp:89-114,
-//                        tgsw-functions.cpp:297-410, tlwe-functions.cpp:202-206)
+//   (the blind rotation itself lives in blind_rotate.cu)
 //   extract_kernel       sample extraction at index 0, MUX recombination   (lwe.cpp:41-60,
 //                        boot-gates.cpp:360-364)
 //   keyswitch_kernel     integer gather-accumulate keyswitch               (lwe-keyswitch-functions.cpp:114-238)
@@ -52,280 +48,6 @@ cudaError_t launch_prologue(const tfheb_params &p, const BootDesc *d_desc, int b
     const uint64_t interv = ((UINT64_C(1) << 63) / (uint64_t)(2 * p.N)) * 2;
     prologue_kernel<<<boots, 256, 0, s>>>(d_desc, a, b ? b : a, c ? c : a, p.n, interv, bara, bara_stride);
     return cudaGetLastError();
-}
-
-// ============================================================================================
-// blind rotation
-// ============================================================================================
-
-// Shared-memory plan of one CTA (GPB teams, one bootstrap per team).
-template <typename T, int N, int K>
-struct BrSmem {
-    static constexpr int M = N / 2;
-    static constexpr int NT = M / kR;
-    static constexpr int TW = tw_offset<M>(FftPlan<M>::NS);         // stage twiddles
-    static constexpr size_t tables_bytes = sizeof(cplx<T>) * (TW + kR * NT);
-    static constexpr size_t team_acc = sizeof(int32_t) * (K + 1) * N;
-    static constexpr size_t team_buf = 2 * sizeof(T) * M;
-    __host__ __device__ static size_t team_bytes(int n) { return team_acc + team_buf + sizeof(int32_t) * ((n + 4) & ~3); }
-    __host__ __device__ static size_t bytes(int gpb, int n) { return tables_bytes + gpb * team_bytes(n); }
-};
-
-// (X^a - 1) * acc, coefficient j (toruspolynomial-functions.cpp:117-136), 0 <= a < 2N
-template <int N>
-__device__ __forceinline__ uint32_t rot_minus_one(const uint32_t *poly, int j, int a) {
-    int src = j - a;
-    uint32_t v;
-    if (src >= 0) v = poly[src];
-    else if (src >= -N) v = 0u - poly[src + N];
-    else v = poly[src + 2 * N];
-    return v - poly[j];
-}
-
-template <typename T>
-__device__ __forceinline__ int64_t round_to_i64(T v);
-template <>
-__device__ __forceinline__ int64_t round_to_i64<double>(double v) { return __double2ll_rn(v); }
-template <>
-__device__ __forceinline__ int64_t round_to_i64<float>(float v) { return __float2ll_rn(v); }
-
-// Bootstrapping-key slot loads (16 bytes per slot).
-template <typename T, bool SPLIT>
-struct BskSlot;
-template <>
-struct BskSlot<double, false> {
-    cplx<double> v;
-    __device__ __forceinline__ void load(const void *base, size_t idx) {
-        const double2 d = __ldg(reinterpret_cast<const double2 *>(base) + idx);
-        v = {d.x, d.y};
-    }
-};
-template <>
-struct BskSlot<float, true> {
-    cplx<float> hi, lo;
-    __device__ __forceinline__ void load(const void *base, size_t idx) {
-        const float4 d = __ldg(reinterpret_cast<const float4 *>(base) + idx);
-        hi = {d.x, d.y};
-        lo = {d.z, d.w};
-    }
-};
-
-template <typename T, int N, int K, int L, bool SPLIT, int GPB>
-__global__ void __launch_bounds__(GPB *(N / 2 / kR))
-    blind_rotate_kernel(const int32_t *__restrict__ bara, int bara_stride, const void *__restrict__ bsk,
-                        const cplx<T> *__restrict__ tables, const int32_t *__restrict__ acc_in,
-                        int32_t *__restrict__ acc_out, int boots, int nsteps, int32_t mu, int Bgbit,
-                        int split_shift) {
-    constexpr int M = N / 2, NT = M / kR, KP1 = K + 1, KPL = KP1 * L;
-    using Sm = BrSmem<T, N, K>;
-    using F = TeamFft<T, M, kR>;
-    extern __shared__ __align__(16) unsigned char smem[];
-
-    // ---- CTA-wide: tables to shared memory ------------------------------------------------
-    cplx<T> *s_tables = reinterpret_cast<cplx<T> *>(smem);
-    for (int i = threadIdx.x; i < Sm::TW + kR * NT; i += blockDim.x) s_tables[i] = tables[i];
-    __syncthreads();
-    const cplx<T> *s_tw = s_tables;
-    const cplx<T> *s_twist = s_tables + Sm::TW;
-
-    const int team = threadIdx.x / NT;
-    const int t = threadIdx.x - team * NT;
-    const int boot = blockIdx.x * GPB + team;
-    if (boot >= boots) return;  // whole team leaves; no CTA-wide barrier follows
-    const int bar_id = 1 + team;
-
-    unsigned char *tb = smem + Sm::tables_bytes + (size_t)team * Sm::team_bytes(nsteps);
-    uint32_t *s_acc = reinterpret_cast<uint32_t *>(tb);
-    T *buf_re = reinterpret_cast<T *>(tb + Sm::team_acc);
-    T *buf_im = buf_re + M;
-    int32_t *s_bara = reinterpret_cast<int32_t *>(tb + Sm::team_acc + Sm::team_buf);
-
-    // ---- team init: bara row, accumulator ------------------------------------------------
-    const int32_t *my_bara = bara + (size_t)boot * bara_stride;
-    for (int i = t; i < nsteps; i += NT) s_bara[i] = my_bara[i];
-    if (acc_in) {
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(acc_in) + (size_t)boot * KP1 * N;
-        for (int i = t; i < KP1 * N; i += NT) s_acc[i] = src[i];
-    } else {
-        // acc = (0, X^{2N-barb} * [mu,...,mu])  (lwe-bootstrapping-functions-fft.cpp:142-145)
-        const int barb = my_bara[nsteps];
-        const int e = 2 * N - barb;
-        for (int i = t; i < K * N; i += NT) s_acc[i] = 0u;
-        for (int j = t; j < N; j += NT) {
-            int src = j - e;
-            uint32_t neg = 0;
-            while (src < 0) {
-                src += N;
-                neg ^= 1u;
-            }
-            s_acc[K * N + j] = neg ? 0u - (uint32_t)mu : (uint32_t)mu;
-        }
-    }
-    team_sync(bar_id, NT);
-
-    // gadget constants (tgsw.cpp:7-29)
-    uint32_t offset = 0;
-#pragma unroll
-    for (int q = 0; q < L; q++) offset += 1u << (32 - (q + 1) * Bgbit);
-    offset *= 1u << (Bgbit - 1);
-    const uint32_t maskBg = (1u << Bgbit) - 1u;
-    const int32_t halfBg = 1 << (Bgbit - 1);
-
-    cplx<T> twist[kR];
-#pragma unroll
-    for (int r = 0; r < kR; r++) twist[r] = s_twist[r * NT + t];
-
-    for (int step = 0; step < nsteps; step++) {
-        const int ai = s_bara[step] & (2 * N - 1);  // rotations live in Z_2N; keeps indices in bounds
-        cplx<T> acc_hi[KP1][kR];
-        cplx<T> acc_lo[SPLIT ? KP1 : 1][kR];
-#pragma unroll
-        for (int v = 0; v < KP1; v++)
-#pragma unroll
-            for (int r = 0; r < kR; r++) {
-                acc_hi[v][r] = {T(0), T(0)};
-                if (SPLIT) acc_lo[SPLIT ? v : 0][r] = {T(0), T(0)};
-            }
-
-        const size_t bsk_step = (size_t)step * KPL * KP1 * kR * NT;
-#pragma unroll 1
-        for (int u = 0; u < KP1; u++) {
-            const uint32_t *poly = s_acc + u * N;
-            uint32_t x0[kR], x1[kR];
-#pragma unroll
-            for (int r = 0; r < kR; r++) {
-                const int j = t + NT * r;
-                x0[r] = rot_minus_one<N>(poly, j, ai) + offset;
-                x1[r] = rot_minus_one<N>(poly, j + M, ai) + offset;
-            }
-#pragma unroll 1
-            for (int q = 0; q < L; q++) {
-                const int shift = 32 - (q + 1) * Bgbit;
-                cplx<T> z[kR];
-#pragma unroll
-                for (int r = 0; r < kR; r++) {
-                    const int32_t d0 = (int32_t)((x0[r] >> shift) & maskBg) - halfBg;
-                    const int32_t d1 = (int32_t)((x1[r] >> shift) & maskBg) - halfBg;
-                    // (a_j - i a_{j+M}) * exp(-i pi j / N)
-                    z[r] = cmul(cplx<T>{T(d0), T(-d1)}, twist[r]);
-                }
-                F::forward(z, buf_re, buf_im, s_tw, t, bar_id);
-                const int p = u * L + q;
-#pragma unroll
-                for (int v = 0; v < KP1; v++) {
-                    const size_t base = bsk_step + ((size_t)p * KP1 + v) * kR * NT + t;
-#pragma unroll
-                    for (int r = 0; r < kR; r++) {
-                        BskSlot<T, SPLIT> s;
-                        s.load(bsk, base + (size_t)r * NT);
-                        if constexpr (SPLIT) {
-                            cmac(acc_hi[v][r], z[r], s.hi);
-                            cmac(acc_lo[v][r], z[r], s.lo);
-                        } else {
-                            cmac(acc_hi[v][r], z[r], s.v);
-                        }
-                    }
-                }
-            }
-        }
-
-        // inverse transforms and accumulate (the key was pre-scaled by 1/M)
-#pragma unroll
-        for (int v = 0; v < KP1; v++) {
-            uint32_t c0[kR], c1[kR];
-            {
-                cplx<T> z[kR];
-#pragma unroll
-                for (int r = 0; r < kR; r++) z[r] = acc_hi[v][r];
-                F::inverse(z, buf_re, buf_im, s_tw, t, bar_id);
-#pragma unroll
-                for (int r = 0; r < kR; r++) {
-                    const cplx<T> w = cmulconj(z[r], twist[r]);  // (c_j - i c_{j+M})
-                    const uint64_t lo0 = (uint64_t)round_to_i64<T>(w.re);
-                    const uint64_t lo1 = (uint64_t)round_to_i64<T>(-w.im);
-                    if constexpr (SPLIT) {
-                        c0[r] = (uint32_t)lo0 << split_shift;
-                        c1[r] = (uint32_t)lo1 << split_shift;
-                    } else {
-                        c0[r] = (uint32_t)lo0;
-                        c1[r] = (uint32_t)lo1;
-                    }
-                }
-            }
-            if constexpr (SPLIT) {
-                cplx<T> z[kR];
-#pragma unroll
-                for (int r = 0; r < kR; r++) z[r] = acc_lo[v][r];
-                F::inverse(z, buf_re, buf_im, s_tw, t, bar_id);
-#pragma unroll
-                for (int r = 0; r < kR; r++) {
-                    const cplx<T> w = cmulconj(z[r], twist[r]);
-                    c0[r] += (uint32_t)(uint64_t)round_to_i64<T>(w.re);
-                    c1[r] += (uint32_t)(uint64_t)round_to_i64<T>(-w.im);
-                }
-            }
-            uint32_t *poly = s_acc + v * N;
-#pragma unroll
-            for (int r = 0; r < kR; r++) {
-                const int j = t + NT * r;
-                poly[j] += c0[r];
-                poly[j + M] += c1[r];
-            }
-        }
-        team_sync(bar_id, NT);
-    }
-
-    uint32_t *dst = reinterpret_cast<uint32_t *>(acc_out) + (size_t)boot * KP1 * N;
-    for (int i = t; i < KP1 * N; i += NT) dst[i] = s_acc[i];
-}
-
-template <typename T, int N, int K, int L, bool SPLIT, int GPB>
-static cudaError_t launch_br_t(const DeviceBsk &bsk, const int32_t *bara, int bara_stride, int boots, int nsteps,
-                               int32_t mu, const int32_t *acc_in, int32_t *acc_out, int Bgbit, cudaStream_t s) {
-    constexpr int NT = N / 2 / kR;
-    const size_t smem = BrSmem<T, N, K>::bytes(GPB, nsteps);
-    auto kern = blind_rotate_kernel<T, N, K, L, SPLIT, GPB>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    const int grid = (boots + GPB - 1) / GPB;
-    kern<<<grid, GPB * NT, smem, s>>>(bara, bara_stride, bsk.bsk, reinterpret_cast<const cplx<T> *>(bsk.tables),
-                                      acc_in, acc_out, boots, nsteps, mu, Bgbit, bsk.split_shift);
-    return cudaGetLastError();
-}
-
-int blind_rotate_supported(const tfheb_params &p) {
-    // teams of N/16 threads synchronise with named barriers, which need whole warps: N >= 512
-    if (p.k != 1 || p.l != 3) return 0;
-    return p.N == 512 || p.N == 1024 || p.N == 2048;
-}
-
-template <int N>
-static cudaError_t launch_br_n(int precision, const DeviceBsk &bsk, const int32_t *bara, int bara_stride,
-                               int boots, int nsteps, int32_t mu, const int32_t *acc_in, int32_t *acc_out, int Bgbit,
-                               cudaStream_t s, int gpb) {
-    if (precision == TFHEB_FP64) {
-        if (gpb >= 2)
-            return launch_br_t<double, N, 1, 3, false, 2>(bsk, bara, bara_stride, boots, nsteps, mu, acc_in, acc_out,
-                                                         Bgbit, s);
-        return launch_br_t<double, N, 1, 3, false, 1>(bsk, bara, bara_stride, boots, nsteps, mu, acc_in, acc_out,
-                                                     Bgbit, s);
-    }
-    if (gpb >= 2)
-        return launch_br_t<float, N, 1, 3, true, 2>(bsk, bara, bara_stride, boots, nsteps, mu, acc_in, acc_out, Bgbit,
-                                                   s);
-    return launch_br_t<float, N, 1, 3, true, 1>(bsk, bara, bara_stride, boots, nsteps, mu, acc_in, acc_out, Bgbit, s);
-}
-
-cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const DeviceBsk &bsk, const int32_t *bara,
-                                int bara_stride, int boots, int nsteps, int32_t mu, const int32_t *acc_in,
-                                int32_t *acc_out, cudaStream_t s, int gpb) {
-    if (boots <= 0) return cudaSuccess;
-    switch (p.N) {
-        case 512: return launch_br_n<512>(precision, bsk, bara, bara_stride, boots, nsteps, mu, acc_in, acc_out, p.Bgbit, s, gpb);
-        case 1024: return launch_br_n<1024>(precision, bsk, bara, bara_stride, boots, nsteps, mu, acc_in, acc_out, p.Bgbit, s, gpb);
-        case 2048: return launch_br_n<2048>(precision, bsk, bara, bara_stride, boots, nsteps, mu, acc_in, acc_out, p.Bgbit, s, gpb);
-        default: return cudaErrorInvalidValue;
-    }
 }
 
 // ============================================================================================
