@@ -67,8 +67,9 @@ __device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void *src, uin
 }
 
 // Bounded wait: true when the phase completed, false on timeout or when the CTA already aborted.
+// The thread whose wait runs out raises the CTA's abort flag and the launch's error word.
 __device__ __forceinline__ bool wait_bounded(uint32_t bar, uint32_t parity, volatile int32_t *abort_flag,
-                                             uint64_t timeout_ns) {
+                                             uint64_t timeout_ns, int32_t *err) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_timer_ns();
     for (;;) {
@@ -76,6 +77,7 @@ __device__ __forceinline__ bool wait_bounded(uint32_t bar, uint32_t parity, vola
         if (mbar_try_wait(bar, parity)) return true;
         if (global_timer_ns() - t0 > timeout_ns) {
             *abort_flag = 1;
+            atomicOr(err, 1);
             return false;
         }
     }
@@ -203,7 +205,8 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
             if (!args.stall_producer) {
                 for (int c = 0; c < total_chunks; c++) {
                     const int s = c % D;
-                    if (c >= D && !wait_bounded(empty_bar(s), ((c / D) - 1) & 1, abort_flag, args.timeout_ns)) break;
+                    if (c >= D && !wait_bounded(empty_bar(s), ((c / D) - 1) & 1, abort_flag, args.timeout_ns, args.err))
+                        break;
                     mbar_arrive_expect_tx(full_bar(s), Lay::chunk);
                     bulk_copy_g2s(ring + (uint32_t)s * Lay::chunk, args.bsk + (size_t)c * Lay::chunk, Lay::chunk,
                                   full_bar(s));
@@ -213,8 +216,7 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
             // drain the copies still in flight before the CTA may exit (each wait bounded)
             volatile int32_t no_abort = 0;
             for (int c = (issued > D ? issued - D : 0); c < issued; c++)
-                wait_bounded(full_bar(c % D), (c / D) & 1, &no_abort, args.timeout_ns);
-            if (*abort_flag) atomicOr(args.err, 1);
+                wait_bounded(full_bar(c % D), (c / D) & 1, &no_abort, args.timeout_ns, args.err);
         }
         return;
     }
@@ -300,7 +302,7 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                 F::forward(z, buf_re, buf_im, s_tw, t, bar_id);
 
                 const int s = c % D;
-                wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns);
+                wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns, args.err);
                 const unsigned char *stage = smem + Lay::ring + (size_t)s * Lay::chunk;
 #pragma unroll
                 for (int v = 0; v < KP1; v++)
