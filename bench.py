@@ -237,6 +237,11 @@ def main():
         return {"total_ms": float(t.item()), "errors": errors, "launches": launches,
                 "kernel_ms": [kms[i] / max(1, kn[i]) for i in range(4)], "kernel_n": [kn[i] for i in range(4)]}
 
+    # pick the fastest compiled blind-rotation launch variant for this batch (both precisions)
+    tuning = {}
+    for name, prec in (("split", tb.SPLIT_FP32), ("fp64", tb.FP64)):
+        tuning[name] = ck.autotune(prec, boots=B)
+
     # FMA throughput probe (roofline denominator at the current clocks)
     peak = {}
     for name, prec in (("fp32", tb.SPLIT_FP32), ("fp64", tb.FP64)):
@@ -307,6 +312,7 @@ def main():
                          "traffic": traffic,
                          "algorithmic": f"{FLOPS_PER_GATE[args.form] / 1e6:.2f} MFLOP/gate x {B} gates per launch"},
             "peaks_measured": peak,
+            "autotune": {k: [{"teams_per_cta": g, "ring_depth": d, "ms": m} for g, d, m in v] for k, v in tuning.items()},
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * B * (p.n + 1) * 4,
                     "d2h_bytes_per_step": B * (p.n + 1) * 4, "errors": e2e_errors,

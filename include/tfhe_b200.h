@@ -168,6 +168,16 @@ tfheb_status tfheb_profile_read(tfheb_cloud_key *ck, double *ms, int64_t *launch
  * measured by a dependent-chain probe kernel: the CUDA-core roofline denominator. */
 tfheb_status tfheb_measure_fma_peak(int32_t device, int32_t precision, double *tflops);
 
+/* Blind-rotation launch variants compiled for ring degree N and a precision: bootstraps per CTA
+ * (teams_per_cta) and key-ring depth; *count receives how many exist (arrays filled up to cap).
+ * tfheb_set_br_variant picks one for a key; tfheb_autotune times them all on `boots` synthetic
+ * bootstraps, keeps the fastest for the key, and writes each variant's time to ms[] (up to cap).
+ * No reference counterpart (the reference has one CPU code path). */
+tfheb_status tfheb_br_variants(int32_t N, int32_t precision, int32_t *teams_per_cta, int32_t *ring_depth,
+                               int32_t cap, int32_t *count);
+tfheb_status tfheb_set_br_variant(tfheb_cloud_key *ck, int32_t precision, int32_t variant);
+tfheb_status tfheb_autotune(tfheb_cloud_key *ck, int32_t precision, int32_t boots, double *ms, int32_t cap);
+
 /* Weight exponent S of the high limb the split-FP32 key uses by default for a parameter set. */
 int32_t tfheb_default_split_shift(const tfheb_params *p);
 

@@ -72,6 +72,9 @@ def lib():
         L.tfheb_set_wait_timeout.argtypes = [_V, ctypes.c_uint64]
         L.tfheb_test_stall_key_stream.argtypes = [_V, _I32]
         L.tfheb_fft_slot_order.argtypes = [_I32, _V]
+        L.tfheb_br_variants.argtypes = [_I32, _I32, _V, _V, _I32, _V]
+        L.tfheb_set_br_variant.argtypes = [_V, _I32, _I32]
+        L.tfheb_autotune.argtypes = [_V, _I32, _I32, _V, _I32]
         _lib = L
     return _lib
 
@@ -211,6 +214,16 @@ class CloudKey:
     def keyswitch_device(self, d_in, d_out, count, stream=None):
         _check(lib().tfheb_keyswitch_device(self.h, count, _p(d_in), _p(d_out), stream), "tfheb_keyswitch_device")
 
+    def autotune(self, precision, boots=4096):
+        """Times every compiled blind-rotation variant; returns [(teams_per_cta, ring_depth, ms)]."""
+        G, D = br_variants(self.params.N, precision)
+        ms = np.zeros(len(G), np.float64)
+        _check(lib().tfheb_autotune(self.h, precision, boots, _p(ms), len(G)), "tfheb_autotune")
+        return list(zip(G.tolist(), D.tolist(), ms.tolist()))
+
+    def set_br_variant(self, precision, variant):
+        _check(lib().tfheb_set_br_variant(self.h, precision, variant), "tfheb_set_br_variant")
+
     def set_wait_timeout(self, seconds):
         _check(lib().tfheb_set_wait_timeout(self.h, ctypes.c_uint64(int(seconds * 1e9))), "tfheb_set_wait_timeout")
 
@@ -236,6 +249,14 @@ def keygen(params, seed=1):
     sk, ck = _V(), _V()
     _check(lib().tfheb_keygen(ctypes.byref(params), seed, ctypes.byref(sk), ctypes.byref(ck)), "tfheb_keygen")
     return SecretKey(sk.value, params), CloudKey(ck.value, params)
+
+
+def br_variants(N, precision):
+    cnt = ctypes.c_int32()
+    G = np.zeros(16, np.int32)
+    D = np.zeros(16, np.int32)
+    _check(lib().tfheb_br_variants(N, precision, _p(G), _p(D), 16, ctypes.byref(cnt)), "tfheb_br_variants")
+    return G[:cnt.value], D[:cnt.value]
 
 
 def fft_slot_order(N):

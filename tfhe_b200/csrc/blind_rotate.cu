@@ -129,7 +129,7 @@ struct BrLayout {
     static constexpr size_t bars = 0;                           // full[D], empty[D], abort flag
     static constexpr size_t ring = 128;
     static constexpr size_t tables = ring + (size_t)D * chunk;
-    static constexpr size_t tables_bytes = ((sizeof(cplx<T>) * (TW + kR * NT)) + 15) / 16 * 16;
+    static constexpr size_t tables_bytes = ((sizeof(cplx<T>) * TW) + 15) / 16 * 16;
     static constexpr size_t teams = tables + tables_bytes;
     static constexpr size_t team_acc = 4 * (size_t)KP1 * N;
     static constexpr size_t team_buf = 2 * sizeof(T) * M;
@@ -156,15 +156,13 @@ struct BrArgs {
     int stall_producer;
 };
 
-// (X^a - 1) * acc, coefficient j (toruspolynomial-functions.cpp:117-136), 0 <= a < 2N
+// (X^a - 1) * acc, coefficient j (toruspolynomial-functions.cpp:117-136), 0 <= a < 2N, without
+// branches: e = (j - a) mod 2N selects coefficient e mod N, negated when e >= N (X^N = -1).
 template <int N>
 __device__ __forceinline__ uint32_t rot_minus_one(const uint32_t *poly, int j, int a) {
-    const int src = j - a;
-    uint32_t v;
-    if (src >= 0) v = poly[src];
-    else if (src >= -N) v = 0u - poly[src + N];
-    else v = poly[src + 2 * N];
-    return v - poly[j];
+    const int e = (j - a) & (2 * N - 1);
+    const uint32_t neg = 0u - (uint32_t)((e & N) != 0);
+    return ((poly[e & (N - 1)] ^ neg) - neg) - poly[j];
 }
 
 template <typename T, int N, int K, int L, bool SPLIT, int G, int D>
@@ -193,7 +191,7 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
     }
     cplx<T> *s_tab = reinterpret_cast<cplx<T> *>(smem + Lay::tables);
     const cplx<T> *g_tab = reinterpret_cast<const cplx<T> *>(args.tables);
-    for (int i = tid; i < Lay::TW + kR * NT; i += blockDim.x) s_tab[i] = g_tab[i];
+    for (int i = tid; i < Lay::TW; i += blockDim.x) s_tab[i] = g_tab[i];
     __syncthreads();
 
     const int total_chunks = args.nsteps * KPL;
@@ -230,11 +228,9 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
 
     unsigned char *tb = smem + Lay::teams + (size_t)team * Lay::team_bytes(args.nsteps);
     uint32_t *s_acc = reinterpret_cast<uint32_t *>(tb);
-    T *buf_re = reinterpret_cast<T *>(tb + Lay::team_acc);
-    T *buf_im = buf_re + M;
+    cplx<T> *buf = reinterpret_cast<cplx<T> *>(tb + Lay::team_acc);
     int32_t *s_bara = reinterpret_cast<int32_t *>(tb + Lay::team_acc + Lay::team_buf);
     const cplx<T> *s_tw = s_tab;
-    const cplx<T> *s_twist = s_tab + Lay::TW;
 
     const int32_t *my_bara = args.bara + (size_t)boot * args.bara_stride;
     for (int i = t; i < args.nsteps; i += NT) s_bara[i] = my_bara[i];
@@ -297,9 +293,9 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                 for (int r = 0; r < kR; r++) {
                     const T d0 = DigitConv<T>::conv((x0[r] >> shift) & maskBg, digit_bias);
                     const T d1 = DigitConv<T>::conv((x1[r] >> shift) & maskBg, digit_bias);
-                    z[r] = cmul(cplx<T>{d0, -d1}, s_twist[r * NT + t]);  // (a_j - i a_{j+M}) e^{-i pi j/N}
+                    z[r] = cplx<T>{d0, -d1};  // a_j - i a_{j+M}; the twist is folded into the FFT
                 }
-                F::forward(z, buf_re, buf_im, s_tw, t, bar_id);
+                F::forward(z, buf, s_tw, t, bar_id);
 
                 const int s = c % D;
                 wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns, args.err);
@@ -330,10 +326,10 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                 cplx<T> z[kR];
 #pragma unroll
                 for (int r = 0; r < kR; r++) z[r] = acc_hi[v][r];
-                F::inverse(z, buf_re, buf_im, s_tw, t, bar_id);
+                F::inverse(z, buf, s_tw, t, bar_id);
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
-                    const cplx<T> w = cmulconj(z[r], s_twist[r * NT + t]);  // (c_j - i c_{j+M})
+                    const cplx<T> w = z[r];  // (c_j - i c_{j+M})
                     if constexpr (SPLIT) {
                         c0[r] = round_f32_mod32(w.re) << args.split_shift;
                         c1[r] = round_f32_mod32(-w.im) << args.split_shift;
@@ -347,10 +343,10 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                 cplx<T> z[kR];
 #pragma unroll
                 for (int r = 0; r < kR; r++) z[r] = acc_lo[SPLIT ? v : 0][r];
-                F::inverse(z, buf_re, buf_im, s_tw, t, bar_id);
+                F::inverse(z, buf, s_tw, t, bar_id);
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
-                    const cplx<T> w = cmulconj(z[r], s_twist[r * NT + t]);
+                    const cplx<T> w = z[r];
                     c0[r] += (uint32_t)__float2ll_rn(w.re);
                     c1[r] += (uint32_t)__float2ll_rn(-w.im);
                 }
@@ -389,27 +385,55 @@ int blind_rotate_supported(const tfheb_params &p) {
     return p.N == 512 || p.N == 1024 || p.N == 2048;
 }
 
-// bootstraps per CTA for (N, precision); each variant's shared memory stays within 227 KB
-int br_teams_per_cta(int N, int precision) {
-    if (N == 2048) return precision == TFHEB_FP64 ? 2 : 3;
-    if (N == 1024) return precision == TFHEB_FP64 ? 4 : 7;
-    return 8;
+// Compiled launch variants: (ring degree, precision, bootstraps per CTA G, key-ring depth D).
+// Every variant's shared memory stays within 227 KB.  The first variant of a (N, precision) pair is
+// the default; tfheb_autotune times all of them on the device and keeps the fastest per key.
+struct BrVariant {
+    int N, precision, G, D;
+    cudaError_t (*launch)(const BrArgs &, cudaStream_t);
+};
+static const BrVariant kBrVariants[] = {
+    {1024, TFHEB_SPLIT_FP32, 7, 4, launch_g<float, 1024, true, 7, 4>},
+    {1024, TFHEB_SPLIT_FP32, 5, 4, launch_g<float, 1024, true, 5, 4>},
+    {1024, TFHEB_SPLIT_FP32, 4, 4, launch_g<float, 1024, true, 4, 4>},
+    {1024, TFHEB_FP64, 3, 4, launch_g<double, 1024, false, 3, 4>},
+    {1024, TFHEB_FP64, 4, 4, launch_g<double, 1024, false, 4, 4>},
+    {1024, TFHEB_FP64, 2, 4, launch_g<double, 1024, false, 2, 4>},
+    {2048, TFHEB_SPLIT_FP32, 3, 3, launch_g<float, 2048, true, 3, 3>},
+    {2048, TFHEB_SPLIT_FP32, 2, 3, launch_g<float, 2048, true, 2, 3>},
+    {2048, TFHEB_FP64, 2, 3, launch_g<double, 2048, false, 2, 3>},
+    {2048, TFHEB_FP64, 1, 4, launch_g<double, 2048, false, 1, 4>},
+    {512, TFHEB_SPLIT_FP32, 8, 4, launch_g<float, 512, true, 8, 4>},
+    {512, TFHEB_FP64, 8, 4, launch_g<double, 512, false, 8, 4>},
+};
+
+int br_variants(int N, int precision, int *G, int *D, int cap) {
+    int n = 0;
+    for (const auto &v : kBrVariants)
+        if (v.N == N && v.precision == precision) {
+            if (n < cap) {
+                if (G) G[n] = v.G;
+                if (D) D[n] = v.D;
+            }
+            n++;
+        }
+    return n;
 }
 
 cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const DeviceBsk &bsk, const int32_t *bara,
                                 int bara_stride, int boots, int nsteps, int32_t mu, const int32_t *acc_in,
                                 int32_t *acc_out, cudaStream_t s, int32_t *d_err, int stall_producer,
-                                uint64_t timeout_ns) {
+                                uint64_t timeout_ns, int variant) {
     if (boots <= 0) return cudaSuccess;
     BrArgs a{bara, bara_stride, reinterpret_cast<const uint8_t *>(bsk.bsk), bsk.tables, acc_in, acc_out, boots,
              nsteps, mu, p.Bgbit, bsk.split_shift, d_err, timeout_ns, stall_producer};
-    const bool sp = precision == TFHEB_SPLIT_FP32;
-    switch (p.N) {
-        case 512: return sp ? launch_g<float, 512, true, 8, 4>(a, s) : launch_g<double, 512, false, 8, 4>(a, s);
-        case 1024: return sp ? launch_g<float, 1024, true, 7, 4>(a, s) : launch_g<double, 1024, false, 4, 4>(a, s);
-        case 2048: return sp ? launch_g<float, 2048, true, 3, 3>(a, s) : launch_g<double, 2048, false, 2, 3>(a, s);
-        default: return cudaErrorInvalidValue;
-    }
+    int seen = 0;
+    for (const auto &v : kBrVariants)
+        if (v.N == p.N && v.precision == precision) {
+            if (seen == variant) return v.launch(a, s);
+            seen++;
+        }
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace tfheb

@@ -162,7 +162,7 @@ static tfheb_status run_pipeline(CloudKey &ck, int precision, int count, int boo
     TFHEB_CUDA(timed(ck, 1, s, [&] {
         return launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, boots, p.n,
                                    modswitch_to_torus32(1, 8), nullptr, ck.d_acc, s, ck.d_err, ck.stall_producer,
-                                   ck.wait_timeout_ns);
+                                   ck.wait_timeout_ns, ck.br_variant[precision]);
     }));
     TFHEB_CUDA(timed(ck, 2, s, [&] { return launch_extract(p, ck.d_gdesc, count, ck.d_acc, ck.d_ksin, kN1, s); }));
     TFHEB_CUDA(timed(ck, 3, s, [&] {
@@ -492,7 +492,8 @@ tfheb_status tfheb_bootstrap_woks_device(tfheb_cloud_key *c, int32_t precision, 
     if ((st = grow(ck.d_acc, ck.acc_cap, (size_t)count * (p.k + 1) * p.N)) != TFHEB_OK) return st;
     TFHEB_CUDA(launch_prologue(p, ck.d_bdesc, count, d_in, d_in, d_in, ck.d_bara, bs, s));
     TFHEB_CUDA(launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, count, p.n, mu, nullptr,
-                                   ck.d_acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns));
+                                   ck.d_acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns,
+                                   ck.br_variant[precision]));
     TFHEB_CUDA(launch_extract(p, ck.d_gdesc, count, ck.d_acc, d_out, p.k * p.N + 1, s));
     g_launches += 3;
     return TFHEB_OK;
@@ -528,7 +529,8 @@ tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *c, int32_t precision, in
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
     // in place: acc_in == acc_out is safe (each team reads its row fully before writing it back)
     TFHEB_CUDA(launch_blind_rotate(ck.p, precision, ck.dbsk[precision], d_bara, nsteps, count, nsteps, 0, d_acc,
-                                   d_acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns));
+                                   d_acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns,
+                                   ck.br_variant[precision]));
     g_launches += 1;
     return TFHEB_OK;
 }
@@ -562,6 +564,70 @@ tfheb_status tfheb_set_wait_timeout(tfheb_cloud_key *c, uint64_t timeout_ns) {
     if (!c || timeout_ns == 0) return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
     c->ck.wait_timeout_ns = timeout_ns;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_br_variants(int32_t N, int32_t precision, int32_t *teams_per_cta, int32_t *ring_depth,
+                               int32_t cap, int32_t *count) {
+    if (!count) return TFHEB_ERR_INVALID;
+    *count = br_variants(N, precision, teams_per_cta, ring_depth, cap);
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_set_br_variant(tfheb_cloud_key *c, int32_t precision, int32_t variant) {
+    if (!c || (precision != TFHEB_FP64 && precision != TFHEB_SPLIT_FP32)) return TFHEB_ERR_INVALID;
+    if (variant < 0 || variant >= br_variants(c->ck.p.N, precision, nullptr, nullptr, 0)) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->ck.br_variant[precision] = variant;
+    return TFHEB_OK;
+}
+
+// Times every compiled blind-rotation variant on `boots` synthetic bootstraps (random rotation
+// amounts, the key's own bootstrapping key) and keeps the fastest for this key and precision.
+tfheb_status tfheb_autotune(tfheb_cloud_key *c, int32_t precision, int32_t boots, double *ms_out, int32_t cap) {
+    if (!c || boots <= 0) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    tfheb_status st = ensure_device(ck, precision);
+    if (st != TFHEB_OK) return st;
+    const tfheb_params &p = ck.p;
+    const int bs = bara_stride_of(p);
+    if ((st = grow(ck.d_bara, ck.bara_cap, (size_t)boots * bs)) != TFHEB_OK) return st;
+    if ((st = grow(ck.d_acc, ck.acc_cap, (size_t)boots * (p.k + 1) * p.N)) != TFHEB_OK) return st;
+    std::vector<int32_t> bara((size_t)boots * bs);
+    uint64_t x = 0x9E3779B97F4A7C15ull;
+    for (auto &v : bara) {
+        x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+        v = (int32_t)(x % (uint64_t)(2 * p.N));
+    }
+    TFHEB_CUDA(cudaMemcpy(ck.d_bara, bara.data(), bara.size() * 4, cudaMemcpyHostToDevice));
+    const int nv = br_variants(p.N, precision, nullptr, nullptr, 0);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = 0;
+    float best_ms = 1e30f;
+    for (int v = 0; v < nv; v++) {
+        float ms = 0;
+        for (int rep = 0; rep < 2; rep++) {  // first run warms up
+            TFHEB_CUDA(cudaEventRecord(e0, ck.stream));
+            TFHEB_CUDA(launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, boots, p.n,
+                                           modswitch_to_torus32(1, 8), nullptr, ck.d_acc, ck.stream, ck.d_err, 0,
+                                           ck.wait_timeout_ns, v));
+            TFHEB_CUDA(cudaEventRecord(e1, ck.stream));
+            TFHEB_CUDA(cudaEventSynchronize(e1));
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (ms_out && v < cap) ms_out[v] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if ((st = check_device_error(ck)) != TFHEB_OK) return st;
+    ck.br_variant[precision] = best;
     return TFHEB_OK;
 }
 

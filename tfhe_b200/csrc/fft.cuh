@@ -154,69 +154,89 @@ struct Stage {
     static constexpr int stride = L / r;
 };
 
-// Stage S stores W_L^{n1*k2} at [(k2-1)*stride + n1] (k2 in [1,r), n1 < stride), packed in order.
+// Twiddle tables, packed per stage.  Stage 0 stores the combined factor
+//     exp(-i pi t / N) * W_M^{t*k2}   at [k2*NT + t], k2 in [0, 8)
+// (the negacyclic twist exp(-i pi j / N), j = t + NT*n2, split as exp(-i pi t/N) * exp(-i pi n2/16):
+// the first factor is common to the thread's eight inputs and moves behind the radix-8 DFT, the
+// second is a compile-time constant applied before it).  Stages S >= 1 store W_L^{n1*k2} at
+// [(k2-1)*stride + n1], k2 in [1, r), n1 < stride.
 template <int M>
 __host__ __device__ constexpr int tw_offset(int S) {
     int off = 0;
     for (int s = 0; s < S; s++) {
         const int L = stage_len<M>(s), r = FftPlan<M>::radix(s);
-        off += (r - 1) * (L / r);
+        off += (s == 0 ? r : r - 1) * (L / r);
     }
     return off;
 }
-// Shared-memory swizzle for the exchange buffer (bank-conflict free for the FP32 patterns).
-__device__ __forceinline__ int swz(int p) { return p ^ ((p >> 3) & 31); }
+
+// exp(-i pi n / 16), n = 0..7: the per-register part of the twist (NT / N = 1/16 for R = 8)
+__host__ __device__ constexpr double fold_cos(int n) {
+    return n == 0 ? 1.0 : n == 1 ? 0.98078528040323044913 : n == 2 ? 0.92387953251128675613
+         : n == 3 ? 0.83146961230254523708 : n == 4 ? 0.70710678118654752440 : n == 5 ? 0.55557023301960222474
+         : n == 6 ? 0.38268343236508977173 : 0.19509032201612826785;
+}
+__host__ __device__ constexpr double fold_sin(int n) { return n == 0 ? 0.0 : fold_cos(8 - n); }
+
+// Shared-memory swizzles of the exchange buffer (complex elements, 8 or 16 bytes).  Both keep an
+// index inside its aligned block of 16 (float) or 8 (double) elements; chosen by simulating every
+// stage's store and load pattern: float2 has at most 2-way conflicts, double2 none.
+template <typename T>
+__device__ __forceinline__ int swz(int p);
+template <>
+__device__ __forceinline__ int swz<float>(int p) { return p ^ (((p >> 3) ^ (p >> 4)) & 15); }
+template <>
+__device__ __forceinline__ int swz<double>(int p) { return p ^ (((p >> 3) + (p >> 6)) & 7); }
 
 // Named barrier over one team (ids 1..15; 0 is __syncthreads).
 __device__ __forceinline__ void team_sync(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Team FFT: T = M/R threads, t in [0,T), registers x[R], exchange buffer buf_re/buf_im (M entries).
+// Team FFT: T = M/R threads, t in [0,T), registers x[R], exchange buffer buf (M complex).
 template <typename T, int M, int R>
 struct TeamFft {
     static constexpr int NT = M / R;  // threads per team
     static constexpr int NS = FftPlan<M>::NS;
+    static_assert(R == 8 && FftPlan<M>::radix(0) == 8, "stage 0 is the thread's own radix-8 DFT");
 
     // position of register (c, n2) of thread t at stage S
     template <int S>
     __device__ static __forceinline__ int pos(int t, int c, int n2) {
-        constexpr int r = Stage<M, S>::r, L = Stage<M, S>::L, st = Stage<M, S>::stride;
+        constexpr int L = Stage<M, S>::L, st = Stage<M, S>::stride;
         const int b = t + NT * c;
         const int q = b / st, n1 = b - q * st;
         return q * L + n1 + st * n2;
     }
 
     template <int S>
-    __device__ static __forceinline__ void store(const cplx<T> *x, T *buf_re, T *buf_im, int t) {
+    __device__ static __forceinline__ void store(const cplx<T> *x, cplx<T> *buf, int t) {
         constexpr int r = Stage<M, S>::r;
 #pragma unroll
         for (int c = 0; c < R / r; c++)
 #pragma unroll
-            for (int n2 = 0; n2 < r; n2++) {
-                const int p = swz(pos<S>(t, c, n2));
-                buf_re[p] = x[c * r + n2].re;
-                buf_im[p] = x[c * r + n2].im;
-            }
+            for (int n2 = 0; n2 < r; n2++) buf[swz<T>(pos<S>(t, c, n2))] = x[c * r + n2];
     }
 
     template <int S>
-    __device__ static __forceinline__ void load(cplx<T> *x, const T *buf_re, const T *buf_im, int t) {
+    __device__ static __forceinline__ void load(cplx<T> *x, const cplx<T> *buf, int t) {
         constexpr int r = Stage<M, S>::r;
 #pragma unroll
         for (int c = 0; c < R / r; c++)
 #pragma unroll
-            for (int n2 = 0; n2 < r; n2++) {
-                const int p = swz(pos<S>(t, c, n2));
-                x[c * r + n2].re = buf_re[p];
-                x[c * r + n2].im = buf_im[p];
-            }
+            for (int n2 = 0; n2 < r; n2++) x[c * r + n2] = buf[swz<T>(pos<S>(t, c, n2))];
     }
 
     template <int S, bool INV>
     __device__ static __forceinline__ void twiddle(cplx<T> *x, const cplx<T> *tw, int t) {
         constexpr int r = Stage<M, S>::r, st = Stage<M, S>::stride;
-        if constexpr (st > 1) {
+        if constexpr (S == 0) {
+#pragma unroll
+            for (int k2 = 0; k2 < r; k2++) {
+                const cplx<T> w = tw[k2 * NT + t];
+                x[k2] = INV ? cmulconj(x[k2], w) : cmul(x[k2], w);
+            }
+        } else if constexpr (st > 1) {
             const cplx<T> *tws = tw + tw_offset<M>(S);
 #pragma unroll
             for (int c = 0; c < R / r; c++) {
@@ -231,47 +251,56 @@ struct TeamFft {
         }
     }
 
+    // x[n] *= exp(-+ i pi n / 16)
+    template <bool INV>
+    __device__ static __forceinline__ void fold_consts(cplx<T> *x) {
+#pragma unroll
+        for (int n = 1; n < R; n++) {
+            const cplx<T> w{T(fold_cos(n)), T(-fold_sin(n))};
+            x[n] = INV ? cmulconj(x[n], w) : cmul(x[n], w);
+        }
+    }
+
     template <int S>
-    __device__ static __forceinline__ void forward_from(cplx<T> *x, T *buf_re, T *buf_im, const cplx<T> *tw,
-                                                        int t, int bar_id) {
+    __device__ static __forceinline__ void forward_from(cplx<T> *x, cplx<T> *buf, const cplx<T> *tw, int t, int bar_id) {
         constexpr int r = Stage<M, S>::r;
 #pragma unroll
         for (int c = 0; c < R / r; c++) dft<T, false, r>(x + c * r);
         twiddle<S, false>(x, tw, t);
         if constexpr (S + 1 < NS) {
-            store<S>(x, buf_re, buf_im, t);
+            store<S>(x, buf, t);
             team_sync(bar_id, NT);
-            load<S + 1>(x, buf_re, buf_im, t);
+            load<S + 1>(x, buf, t);
             team_sync(bar_id, NT);
-            forward_from<S + 1>(x, buf_re, buf_im, tw, t, bar_id);
+            forward_from<S + 1>(x, buf, tw, t, bar_id);
         }
     }
 
     template <int S>
-    __device__ static __forceinline__ void inverse_from(cplx<T> *x, T *buf_re, T *buf_im, const cplx<T> *tw,
-                                                        int t, int bar_id) {
+    __device__ static __forceinline__ void inverse_from(cplx<T> *x, cplx<T> *buf, const cplx<T> *tw, int t, int bar_id) {
         constexpr int r = Stage<M, S>::r;
         twiddle<S, true>(x, tw, t);
 #pragma unroll
         for (int c = 0; c < R / r; c++) dft<T, true, r>(x + c * r);
         if constexpr (S > 0) {
-            store<S>(x, buf_re, buf_im, t);
+            store<S>(x, buf, t);
             team_sync(bar_id, NT);
-            load<S - 1>(x, buf_re, buf_im, t);
+            load<S - 1>(x, buf, t);
             team_sync(bar_id, NT);
-            inverse_from<S - 1>(x, buf_re, buf_im, tw, t, bar_id);
+            inverse_from<S - 1>(x, buf, tw, t, bar_id);
         }
     }
 
-    // natural order in (x[n2] = point t + NT*n2) -> slot order out
-    __device__ static __forceinline__ void forward(cplx<T> *x, T *buf_re, T *buf_im, const cplx<T> *tw, int t,
-                                                   int bar_id) {
-        forward_from<0>(x, buf_re, buf_im, tw, t, bar_id);
+    // Folded negacyclic transform.  In: x[n2] = a_j - i a_{j+M} for j = t + NT*n2 (no twist applied).
+    // Out: the M evaluation points in slot order.
+    __device__ static __forceinline__ void forward(cplx<T> *x, cplx<T> *buf, const cplx<T> *tw, int t, int bar_id) {
+        fold_consts<false>(x);
+        forward_from<0>(x, buf, tw, t, bar_id);
     }
-    // slot order in -> natural order out (unscaled: returns M * the inverse DFT)
-    __device__ static __forceinline__ void inverse(cplx<T> *x, T *buf_re, T *buf_im, const cplx<T> *tw, int t,
-                                                   int bar_id) {
-        inverse_from<NS - 1>(x, buf_re, buf_im, tw, t, bar_id);
+    // Slot order in -> x[n2] = M * (c_j - i c_{j+M}), j = t + NT*n2 (twist removed).
+    __device__ static __forceinline__ void inverse(cplx<T> *x, cplx<T> *buf, const cplx<T> *tw, int t, int bar_id) {
+        inverse_from<NS - 1>(x, buf, tw, t, bar_id);
+        fold_consts<true>(x);
     }
 };
 

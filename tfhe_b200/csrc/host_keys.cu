@@ -215,12 +215,18 @@ template <int M>
 void tables_m(std::vector<double> &tab) {
     constexpr int NT = M / kR, NS = FftPlan<M>::NS, N = 2 * M;
     const int tw = tw_offset<M>(NS);
-    tab.assign(2 * (size_t)(tw + kR * NT), 0.0);
+    tab.assign(2 * (size_t)tw, 0.0);
     auto put = [&](int idx, long double ang_over_pi) {
         tab[2 * idx] = (double)std::cos((long double)M_PI * ang_over_pi);
         tab[2 * idx + 1] = (double)std::sin((long double)M_PI * ang_over_pi);
     };
-    for (int s = 0; s < NS; s++) {
+    // stage 0: exp(-i pi t / N) * W_M^{t k2} = exp(-i pi t (1 + 4 k2) / N), k2 in [0, 8)
+    for (int k2 = 0; k2 < kR; k2++)
+        for (int t = 0; t < NT; t++) {
+            const long e = ((long)t * (1 + 4 * k2)) % (2 * N);
+            put(k2 * NT + t, -(long double)e / (long double)N);
+        }
+    for (int s = 1; s < NS; s++) {
         const int L = stage_len<M>(s), r = FftPlan<M>::radix(s), st = L / r;
         const int off = tw_offset<M>(s);
         for (int k2 = 1; k2 < r; k2++)
@@ -229,11 +235,6 @@ void tables_m(std::vector<double> &tab) {
                 put(off + (k2 - 1) * st + n1, -2.0L * (long double)e / (long double)L);
             }
     }
-    for (int r = 0; r < kR; r++)
-        for (int t = 0; t < NT; t++) {
-            const int j = t + NT * r;  // exp(-i pi j / N)
-            put(tw + r * NT + t, -(long double)j / (long double)N);
-        }
 }
 
 using cd = std::complex<double>;

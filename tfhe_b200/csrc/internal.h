@@ -66,6 +66,7 @@ struct CloudKey {
     int32_t *d_err = nullptr;       // device error word (bounded waits that ran out)
     uint64_t wait_timeout_ns = 1000000000ull;  // limit of every device-side wait
     int stall_producer = 0;         // test hook: the key-streaming warp issues nothing
+    int br_variant[2] = {0, 0};     // chosen blind-rotation launch variant per precision
     int launches = 0;               // kernels launched (for the bench's launch count)
     // optional per-kernel timing with CUDA events on the launching stream
     bool prof = false;
@@ -103,8 +104,9 @@ cudaError_t launch_prologue(const tfheb_params &p, const BootDesc *d_desc, int b
 cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const DeviceBsk &bsk, const int32_t *bara,
                                 int bara_stride, int boots, int nsteps, int32_t mu, const int32_t *acc_in,
                                 int32_t *acc_out, cudaStream_t s, int32_t *d_err, int stall_producer,
-                                uint64_t timeout_ns);
-int br_teams_per_cta(int N, int precision);
+                                uint64_t timeout_ns, int variant);
+// Launch variants compiled for (N, precision): count, and their (G, D) into the arrays (up to cap).
+int br_variants(int N, int precision, int *G, int *D, int cap);
 cudaError_t launch_extract(const tfheb_params &p, const GateDesc *d_desc, int count, const int32_t *acc,
                            int32_t *out, int out_stride, cudaStream_t s);
 cudaError_t launch_keyswitch(const tfheb_params &p, const int32_t *d_ksk, int ks_stride, int count,
