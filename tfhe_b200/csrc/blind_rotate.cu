@@ -132,7 +132,7 @@ struct BrLayout {
     static constexpr size_t tables_bytes = ((sizeof(cplx<T>) * TW) + 15) / 16 * 16;
     static constexpr size_t teams = tables + tables_bytes;
     static constexpr size_t team_acc = 4 * (size_t)KP1 * N;
-    static constexpr size_t team_buf = 2 * sizeof(T) * M;
+    static constexpr size_t team_buf = ((sizeof(cplx<T>) * ExchPad<T>::size(M)) + 15) / 16 * 16;
     __host__ __device__ static size_t team_bytes(int nsteps) {
         return team_acc + team_buf + 16 * (((size_t)nsteps + 4 + 3) / 4);
     }

@@ -178,15 +178,18 @@ __host__ __device__ constexpr double fold_cos(int n) {
 }
 __host__ __device__ constexpr double fold_sin(int n) { return n == 0 ? 0.0 : fold_cos(8 - n); }
 
-// Shared-memory swizzles of the exchange buffer (complex elements, 8 or 16 bytes).  Both keep an
-// index inside its aligned block of 16 (float) or 8 (double) elements; chosen by simulating every
-// stage's store and load pattern: float2 has at most 2-way conflicts, double2 none.
+// Padded index of the exchange buffer (complex elements, 8 or 16 bytes): one pad element every 16
+// (float) or 8 (double) elements.  The padding is affine on every stage's access pattern -- each of a
+// thread's eight addresses is a per-stage base plus a compile-time offset -- and, simulated over all
+// stores and loads of the 8*8*8 and 8*8*8*2 plans, conflict-free for double2 and at most 2-way for
+// float2.
 template <typename T>
-__device__ __forceinline__ int swz(int p);
-template <>
-__device__ __forceinline__ int swz<float>(int p) { return p ^ (((p >> 3) ^ (p >> 4)) & 15); }
-template <>
-__device__ __forceinline__ int swz<double>(int p) { return p ^ (((p >> 3) + (p >> 6)) & 7); }
+struct ExchPad {
+    static constexpr int shift = sizeof(T) == 4 ? 4 : 3;
+    __host__ __device__ static constexpr int size(int M) { return M + (M >> shift); }
+};
+template <typename T>
+__device__ __forceinline__ int swz(int p) { return p + (p >> ExchPad<T>::shift); }
 
 // Named barrier over one team (ids 1..15; 0 is __syncthreads).
 __device__ __forceinline__ void team_sync(int id, int nthreads) {
