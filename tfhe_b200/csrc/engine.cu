@@ -11,18 +11,12 @@
 
 #include "internal.h"
 
-struct tfheb_secret_key {
-    tfheb::SecretKey sk;
-};
-struct tfheb_cloud_key {
-    tfheb::CloudKey ck;
-    std::mutex mu;  // serialises host callers sharing one key (scratch buffers are per key)
-};
 
 namespace tfheb {
 
 static thread_local std::string g_last_error;
-static std::atomic<int64_t> g_launches{0};
+std::atomic<int64_t> g_kernel_launches{0};
+static std::atomic<int64_t> &g_launches = g_kernel_launches;
 
 void set_error(const std::string &msg) { g_last_error = msg; }
 
@@ -58,6 +52,7 @@ static tfheb_status grow(T *&ptr, size_t &cap, size_t need) {
 }
 
 static int bara_stride_of(const tfheb_params &p) { return (p.n + 4) & ~3; }
+int bara_stride_for(const tfheb_params &p) { return bara_stride_of(p); }
 
 // gate linear combinations (boot-gates.cpp:34-319): constant numerator/denominator and weights
 struct GateForm {
@@ -67,6 +62,13 @@ static const GateForm kForms[10] = {
     {1, 8, -1, -1},  {1, 8, 1, 1},   {-1, 8, 1, 1},  {1, 4, 2, 2},  {-1, 4, -2, -2},
     {-1, 8, -1, -1}, {-1, 8, -1, 1}, {-1, 8, 1, -1}, {1, 8, -1, 1}, {1, 8, 1, -1},
 };
+
+void gate_form(int gate, int32_t *cst, int32_t *sa, int32_t *sb) {
+    const GateForm &f = kForms[gate];
+    *cst = modswitch_to_torus32(f.num, f.den);
+    *sa = f.sa;
+    *sb = f.sb;
+}
 
 // Builds bootstrap and gate descriptors for `count` gates with codes gates[g] (or a uniform code),
 // operands addressed by row indices (or the gate index itself when idx arrays are null).
@@ -117,6 +119,8 @@ static tfheb_status ensure_device(CloudKey &ck, int precision) {
     TFHEB_CUDA(cudaSetDevice(ck.device));
     return TFHEB_OK;
 }
+
+tfheb_status prepare_device(CloudKey &ck, int precision) { return ensure_device(ck, precision); }
 
 // Weight 2^S of the high limb in split mode.  The high-limb product must round to the exact
 // integer: its FP32 error is ~4 * 2^-24 * rms(product) with

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -117,7 +119,24 @@ cudaError_t launch_negate(const int32_t *in, int32_t *out, size_t count, cudaStr
 int default_split_shift(const tfheb_params &p);
 cudaError_t measure_fma_peak(int precision, double *tflops);
 
+// ---- helpers shared with the allocation-free entry point (engine.cu) -------------------------
+// Checks that the key is on its device with an FFT-domain key for `precision` and makes that
+// device current.
+tfheb_status prepare_device(CloudKey &ck, int precision);
+// Linear combination of a binary gate (boot-gates.cpp:34-319): constant and operand weights.
+void gate_form(int gate, int32_t *cst, int32_t *sa, int32_t *sb);
+int bara_stride_for(const tfheb_params &p);
+extern std::atomic<int64_t> g_kernel_launches;
+
 // ---- errors ---------------------------------------------------------------------------------
 void set_error(const std::string &msg);
 
 }  // namespace tfheb
+
+struct tfheb_secret_key {
+    tfheb::SecretKey sk;
+};
+struct tfheb_cloud_key {
+    tfheb::CloudKey ck;
+    std::mutex mu;  // serialises host callers sharing one key (scratch buffers are per key)
+};
