@@ -43,7 +43,109 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["nand", "netlist", "mux2048", "errors"], default="nand",
+                    help="nand: the headline line (4096 NAND batches); the others print their own line: "
+                         "netlist = seeded 200-level random circuit through a CUDA graph, mux2048 = 1024 MUX "
+                         "at N=2048, errors = decryption-error count over 10^6 split-FP32 NAND gates")
+    ap.add_argument("--gates", type=int, default=1_000_000, help="gate count of --workload errors")
     return ap.parse_args()
+
+
+def run_extra_workload(args):
+    """Secondary measurements (not the headline line): one JSON line each."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import tfhe_b200 as tb
+    from tfhe_b200.api import Netlist, eval_plain, random_netlist
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    out = {"workload": args.workload}
+    if args.workload == "netlist":
+        p = tb.default_params()
+        sk, ck = tb.keygen(p, seed=4)
+        ck.to_device(0)
+        rng = np.random.default_rng(2024)
+        ni, gates, ia, ib, ic = random_netlist(rng, levels=200, width_lo=16, width_hi=4096)
+        bits = rng.integers(0, 2, ni)
+        truth = eval_plain(ni, gates, ia, ib, ic, bits)
+        wires = torch.zeros((ni + len(gates), p.n + 1), dtype=torch.int32, device="cuda")
+        wires[:ni] = torch.from_numpy(sk.encrypt(bits, seed=3))
+        for prec, name in ((tb.SPLIT_FP32, "split"), (tb.FP64, "fp64")):
+            ck.autotune(prec, boots=2048)
+            nl = Netlist(ck, ni, gates, ia, ib, ic)
+            nl.run(wires, precision=prec, use_graph=True, stream=sptr)  # eager run + capture
+            torch.cuda.synchronize()
+            times = []
+            for _ in range(max(1, args.steps)):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                nl.run(wires, precision=prec, use_graph=True, stream=sptr)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1))
+            got, _ = sk.decrypt(wires.cpu().numpy())
+            ms = float(np.median(times))
+            out[name] = {"gates_per_s": len(gates) / (ms / 1e3), "ms_per_run": ms,
+                         "wrong_wires": int((got != truth).sum()), "levels": nl.info()[0]}
+            nl.free()
+        out.update({"gates": int(len(gates)), "inputs": int(ni),
+                    "mix": "NAND .40 XOR .20 AND .15 OR .15 MUX .10; widths U[16,4096]; 200 levels; "
+                           "operands uniform over the previous two levels",
+                    "timing": "median device time of one CUDA-graph replay (CUDA events)"})
+    elif args.workload == "mux2048":
+        p = tb.large_params()
+        sk, ck = tb.keygen(p, seed=5)
+        ck.to_device(0)
+        B = 1024
+        rng = np.random.default_rng(3)
+        a, b, c = rng.integers(0, 2, (3, B))
+        d = [torch.from_numpy(sk.encrypt(x, seed=i + 1)).cuda() for i, x in enumerate((a, b, c))]
+        dout = torch.zeros_like(d[0])
+        for prec, name in ((tb.SPLIT_FP32, "split"), (tb.FP64, "fp64")):
+            tune = ck.autotune(prec, boots=2 * B)
+            for _ in range(args.warmup):
+                ck.gate_device(tb.api.MUX, d[0], d[1], d[2], dout, B, precision=prec, stream=sptr)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                ck.gate_device(tb.api.MUX, d[0], d[1], d[2], dout, B, precision=prec, stream=sptr)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            got, _ = sk.decrypt(dout.cpu().numpy())
+            out[name] = {"gates_per_s": B / (ms / 1e3), "ms_per_batch": ms,
+                         "errors": int((got != np.where(a == 1, b, c)).sum()), "autotune": tune}
+        out.update({"params": "n=800,N=2048,k=1,l=3,Bgbit=8,ks_t=8,ks_basebit=2", "batch": B,
+                    "split_shift": int(tb.api.lib().tfheb_default_split_shift(ctypes.byref(p)))})
+    else:  # errors
+        p = tb.default_params()
+        sk, ck = tb.keygen(p, seed=6)
+        ck.to_device(0)
+        ck.autotune(tb.SPLIT_FP32, boots=4096)
+        B, total, errors, done = 4096, args.gates, 0, 0
+        rng = np.random.default_rng(11)
+        dout = torch.zeros((B, p.n + 1), dtype=torch.int32, device="cuda")
+        t0 = time.perf_counter()
+        batch = 0
+        while done < total:
+            bits = rng.integers(0, 2, (2, B))
+            da = torch.from_numpy(sk.encrypt(bits[0], seed=2 * batch + 1)).cuda()
+            db = torch.from_numpy(sk.encrypt(bits[1], seed=2 * batch + 2)).cuda()
+            ck.gate_device(tb.api.NAND, da, db, None, dout, B, precision=tb.SPLIT_FP32, stream=sptr)
+            got, _ = sk.decrypt(dout.cpu().numpy())
+            errors += int((got != 1 - (bits[0] & bits[1])).sum())
+            done += B
+            batch += 1
+        out.update({"form": "split-FP32", "gates": done, "decryption_errors": errors, "batches": batch,
+                    "wall_s": time.perf_counter() - t0})
+    print(json.dumps(out), flush=True)
 
 
 class ClockSampler:
@@ -165,6 +267,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload != "nand":
+        if rank == 0:
+            run_extra_workload(args)
         return
 
     import ctypes

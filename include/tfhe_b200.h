@@ -181,6 +181,24 @@ tfheb_status tfheb_autotune(tfheb_cloud_key *ck, int32_t precision, int32_t boot
 /* Weight exponent S of the high limb the split-FP32 key uses by default for a parameter set. */
 int32_t tfheb_default_split_shift(const tfheb_params *p);
 
+/* Levelled netlist evaluation.  No counterpart in the reference, whose callers chain single gate
+ * calls (test-long-run.cpp:61-185, test-addition-boot.cpp).  Wires 0..num_inputs-1 are primary
+ * inputs; gate g (codes as above, topological order) produces wire num_inputs+g and reads wires
+ * in_a[g], in_b[g] (and in_c[g] for MUX; only in_a for NOT/COPY), each below num_inputs+g.
+ * create: levels the gates, uploads per-level descriptors and allocates the scratch of the widest
+ * level.  run: d_wires is a device array [num_inputs+num_gates][n+1] whose input rows the caller
+ * filled; on return (stream-ordered) row num_inputs+g holds gate g's output.  With use_graph, the
+ * first run on a (precision, d_wires) pair evaluates eagerly and captures the level sequence into a
+ * CUDA graph; later runs replay that graph with one launch. */
+typedef struct tfheb_netlist tfheb_netlist;
+tfheb_status tfheb_netlist_create(tfheb_cloud_key *ck, int32_t num_inputs, int32_t num_gates, const int32_t *gates,
+                                  const int32_t *in_a, const int32_t *in_b, const int32_t *in_c,
+                                  tfheb_netlist **out);
+tfheb_status tfheb_netlist_info(const tfheb_netlist *nl, int32_t *num_levels, int32_t *max_width);
+tfheb_status tfheb_netlist_run(tfheb_netlist *nl, int32_t precision, int32_t *d_wires, int32_t use_graph,
+                               void *stream);
+void tfheb_netlist_free(tfheb_netlist *nl);
+
 /* Allocation-free variant of tfheb_gate_batch_device, for callers that cannot call cudaMalloc
  * (while a CUDA graph is being captured, in real-time or signal-handling code that must not enter
  * the allocator, or under a framework that owns all device memory).  No counterpart in the

@@ -251,6 +251,86 @@ def keygen(params, seed=1):
     return SecretKey(sk.value, params), CloudKey(ck.value, params)
 
 
+class Netlist:
+    """Levelled gate netlist on the GPU (tfheb_netlist_*): wires 0..num_inputs-1 are inputs, gate g
+    writes wire num_inputs+g."""
+
+    def __init__(self, ck, num_inputs, gates, in_a, in_b=None, in_c=None):
+        L = lib()
+        L.tfheb_netlist_create.argtypes = [_V, _I32, _I32, _V, _V, _V, _V, ctypes.POINTER(_V)]
+        L.tfheb_netlist_info.argtypes = [_V, _V, _V]
+        L.tfheb_netlist_run.argtypes = [_V, _I32, _I32, _V, _I32, _V]
+        L.tfheb_netlist_free.argtypes = [_V]
+        self.ck = ck
+        self.num_inputs = int(num_inputs)
+        self.gates = _i32(gates)
+        g = len(self.gates)
+        self._a = _i32(in_a)
+        self._b = _i32(in_b if in_b is not None else np.zeros(g))
+        self._c = _i32(in_c if in_c is not None else np.zeros(g))
+        h = _V()
+        _check(L.tfheb_netlist_create(ck.h, self.num_inputs, g, _p(self.gates), _p(self._a), _p(self._b),
+                                      _p(self._c), ctypes.byref(h)), "tfheb_netlist_create")
+        self.h = h
+
+    def info(self):
+        lv, w = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().tfheb_netlist_info(self.h, ctypes.byref(lv), ctypes.byref(w)), "tfheb_netlist_info")
+        return lv.value, w.value
+
+    def run(self, d_wires, precision=FP64, use_graph=True, stream=None):
+        _check(lib().tfheb_netlist_run(self.h, precision, _p(d_wires), 1 if use_graph else 0, stream),
+               "tfheb_netlist_run")
+
+    def free(self):
+        if self.h:
+            lib().tfheb_netlist_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def random_netlist(rng, levels, width_lo, width_hi, mix=None, first_width=None):
+    """Seeded layered netlist: level widths uniform in [width_lo, width_hi]; gate types drawn with
+    the probabilities `mix` ({code: p}); every operand uniform over the previous two levels.
+    Returns (num_inputs, gates, in_a, in_b, in_c)."""
+    mix = mix or {NAND: 0.40, XOR: 0.20, AND: 0.15, OR: 0.15, MUX: 0.10}
+    codes = np.array(list(mix.keys()))
+    probs = np.array(list(mix.values()), dtype=np.float64)
+    probs /= probs.sum()
+    w0 = first_width or int(rng.integers(width_lo, width_hi + 1))
+    spans = [(0, w0)]  # wire ranges of each level
+    gates, ia, ib, ic = [], [], [], []
+    nxt = w0
+    for _ in range(levels):
+        w = int(rng.integers(width_lo, width_hi + 1))
+        lo = spans[-2][0] if len(spans) >= 2 else spans[-1][0]
+        hi = spans[-1][1]
+        gates.append(rng.choice(codes, size=w, p=probs))
+        ia.append(rng.integers(lo, hi, size=w))
+        ib.append(rng.integers(lo, hi, size=w))
+        ic.append(rng.integers(lo, hi, size=w))
+        spans.append((nxt, nxt + w))
+        nxt += w
+    return (w0, np.concatenate(gates).astype(np.int32), np.concatenate(ia).astype(np.int32),
+            np.concatenate(ib).astype(np.int32), np.concatenate(ic).astype(np.int32))
+
+
+def eval_plain(num_inputs, gates, in_a, in_b, in_c, input_bits):
+    """Plaintext evaluation of a netlist (the truth the decrypted wires must equal)."""
+    wires = np.zeros(num_inputs + len(gates), np.int32)
+    wires[:num_inputs] = input_bits
+    for g, code in enumerate(gates):
+        a, b, c = wires[in_a[g]], wires[in_b[g]], wires[in_c[g]]
+        wires[num_inputs + g] = [1 - (a & b), a | b, a & b, a ^ b, 1 - (a ^ b), 1 - (a | b), (1 - a) & b,
+                                 a & (1 - b), (1 - a) | b, a | (1 - b), b if a else c, 1 - a, a][code]
+    return wires
+
+
 def br_variants(N, precision):
     cnt = ctypes.c_int32()
     G = np.zeros(16, np.int32)
