@@ -259,7 +259,7 @@ class Netlist:
         L = lib()
         L.tfheb_netlist_create.argtypes = [_V, _I32, _I32, _V, _V, _V, _V, ctypes.POINTER(_V)]
         L.tfheb_netlist_info.argtypes = [_V, _V, _V]
-        L.tfheb_netlist_run.argtypes = [_V, _I32, _I32, _V, _I32, _V]
+        L.tfheb_netlist_run.argtypes = [_V, _I32, _V, _I32, _V]
         L.tfheb_netlist_free.argtypes = [_V]
         self.ck = ck
         self.num_inputs = int(num_inputs)

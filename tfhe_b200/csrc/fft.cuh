@@ -86,24 +86,29 @@ __device__ __forceinline__ void dft8(cplx<T> *x) {
     dft4<T, INV>(e0, e1, e2, e3);
     dft4<T, INV>(o0, o1, o2, o3);
     const T h = rsqrt2<T>();
-    // o_k *= W8^k (forward W8 = (1-i)/sqrt2; inverse uses the conjugate)
-    cplx<T> w1, w3;
+    // o_k *= W8^k (forward W8 = (1-i)/sqrt2; inverse uses the conjugate); the 1/sqrt2 scaling is
+    // folded into the combining additions as fused multiply-adds: w_k = h * (u_k + i v_k)
+    T u1, v1, u3, v3;
     if (!INV) {
-        w1 = {(o1.re + o1.im) * h, (o1.im - o1.re) * h};
-        w3 = {(o3.im - o3.re) * h, -(o3.re + o3.im) * h};
+        u1 = o1.re + o1.im;
+        v1 = o1.im - o1.re;
+        u3 = o3.im - o3.re;
+        v3 = -(o3.re + o3.im);
     } else {
-        w1 = {(o1.re - o1.im) * h, (o1.re + o1.im) * h};
-        w3 = {-(o3.re + o3.im) * h, (o3.re - o3.im) * h};
+        u1 = o1.re - o1.im;
+        v1 = o1.re + o1.im;
+        u3 = -(o3.re + o3.im);
+        v3 = o3.re - o3.im;
     }
     const cplx<T> w2 = rot_quarter<T, INV>(o2);
     x[0] = cadd(e0, o0);
     x[4] = csub(e0, o0);
-    x[1] = cadd(e1, w1);
-    x[5] = csub(e1, w1);
+    x[1] = {fma(u1, h, e1.re), fma(v1, h, e1.im)};
+    x[5] = {fma(-u1, h, e1.re), fma(-v1, h, e1.im)};
     x[2] = cadd(e2, w2);
     x[6] = csub(e2, w2);
-    x[3] = cadd(e3, w3);
-    x[7] = csub(e3, w3);
+    x[3] = {fma(u3, h, e3.re), fma(v3, h, e3.im)};
+    x[7] = {fma(-u3, h, e3.re), fma(-v3, h, e3.im)};
 }
 
 template <typename T, bool INV, int RADIX>
