@@ -132,7 +132,7 @@ struct BrLayout {
     static constexpr size_t tables_bytes = ((sizeof(cplx<T>) * TW) + 15) / 16 * 16;
     static constexpr size_t teams = tables + tables_bytes;
     static constexpr size_t team_acc = 4 * (size_t)KP1 * N;
-    static constexpr size_t team_buf = ((sizeof(cplx<T>) * ExchPad<T>::size(M)) + 15) / 16 * 16;
+    static constexpr size_t team_buf = ((size_t)Exch<T, M>::bytes + 15) / 16 * 16;
     __host__ __device__ static size_t team_bytes(int nsteps) {
         return team_acc + team_buf + 16 * (((size_t)nsteps + 4 + 3) / 4);
     }
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
 
     unsigned char *tb = smem + Lay::teams + (size_t)team * Lay::team_bytes(args.nsteps);
     uint32_t *s_acc = reinterpret_cast<uint32_t *>(tb);
-    cplx<T> *buf = reinterpret_cast<cplx<T> *>(tb + Lay::team_acc);
+    void *buf = tb + Lay::team_acc;
     int32_t *s_bara = reinterpret_cast<int32_t *>(tb + Lay::team_acc + Lay::team_buf);
     const cplx<T> *s_tw = s_tab;
 

@@ -183,25 +183,48 @@ __host__ __device__ constexpr double fold_cos(int n) {
 }
 __host__ __device__ constexpr double fold_sin(int n) { return n == 0 ? 0.0 : fold_cos(8 - n); }
 
-// Padded index of the exchange buffer (complex elements, 8 or 16 bytes): one pad element every 16
-// (float) or 8 (double) elements.  The padding is affine on every stage's access pattern -- each of a
-// thread's eight addresses is a per-stage base plus a compile-time offset -- and, simulated over all
-// stores and loads of the 8*8*8 and 8*8*8*2 plans, conflict-free for double2 and at most 2-way for
-// float2.
-template <typename T>
-struct ExchPad {
-    static constexpr int shift = sizeof(T) == 4 ? 4 : 3;
-    __host__ __device__ static constexpr int size(int M) { return M + (M >> shift); }
+// Exchange buffer of one team FFT (M complex points), laid out per precision:
+//   double: interleaved double2 with one pad element every 8 -- affine on every stage's access
+//           pattern (each of a thread's eight addresses is a per-stage base plus a compile-time
+//           offset) and, simulated over all stores and loads of the 8*8*8 and 8*8*8*2 plans,
+//           bank-conflict free for 16-byte accesses;
+//   float:  separate re / im arrays of 32-bit words, XOR-swizzled p ^ ((p >> 3) & 31), which is
+//           conflict free for 32-bit accesses (interleaved float2 with any affine padding leaves
+//           2-way conflicts on the stride-8 stage: measured ~9x more conflicts on B200).
+template <typename T, int M>
+struct Exch;
+template <int M>
+struct Exch<double, M> {
+    static constexpr int bytes = 16 * (M + (M >> 3));
+    __device__ static __forceinline__ void put(void *buf, int p, cplx<double> v) {
+        reinterpret_cast<cplx<double> *>(buf)[p + (p >> 3)] = v;
+    }
+    __device__ static __forceinline__ cplx<double> get(const void *buf, int p) {
+        return reinterpret_cast<const cplx<double> *>(buf)[p + (p >> 3)];
+    }
 };
-template <typename T>
-__device__ __forceinline__ int swz(int p) { return p + (p >> ExchPad<T>::shift); }
+template <int M>
+struct Exch<float, M> {
+    static constexpr int bytes = 8 * M;
+    __device__ static __forceinline__ void put(void *buf, int p, cplx<float> v) {
+        float *re = reinterpret_cast<float *>(buf);
+        const int q = p ^ ((p >> 3) & 31);
+        re[q] = v.re;
+        re[M + q] = v.im;
+    }
+    __device__ static __forceinline__ cplx<float> get(const void *buf, int p) {
+        const float *re = reinterpret_cast<const float *>(buf);
+        const int q = p ^ ((p >> 3) & 31);
+        return {re[q], re[M + q]};
+    }
+};
 
 // Named barrier over one team (ids 1..15; 0 is __syncthreads).
 __device__ __forceinline__ void team_sync(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Team FFT: T = M/R threads, t in [0,T), registers x[R], exchange buffer buf (M complex).
+// Team FFT: T = M/R threads, t in [0,T), registers x[R], exchange buffer buf (Exch<T, M>::bytes).
 template <typename T, int M, int R>
 struct TeamFft {
     static constexpr int NT = M / R;  // threads per team
@@ -218,21 +241,21 @@ struct TeamFft {
     }
 
     template <int S>
-    __device__ static __forceinline__ void store(const cplx<T> *x, cplx<T> *buf, int t) {
+    __device__ static __forceinline__ void store(const cplx<T> *x, void *buf, int t) {
         constexpr int r = Stage<M, S>::r;
 #pragma unroll
         for (int c = 0; c < R / r; c++)
 #pragma unroll
-            for (int n2 = 0; n2 < r; n2++) buf[swz<T>(pos<S>(t, c, n2))] = x[c * r + n2];
+            for (int n2 = 0; n2 < r; n2++) Exch<T, M>::put(buf, pos<S>(t, c, n2), x[c * r + n2]);
     }
 
     template <int S>
-    __device__ static __forceinline__ void load(cplx<T> *x, const cplx<T> *buf, int t) {
+    __device__ static __forceinline__ void load(cplx<T> *x, const void *buf, int t) {
         constexpr int r = Stage<M, S>::r;
 #pragma unroll
         for (int c = 0; c < R / r; c++)
 #pragma unroll
-            for (int n2 = 0; n2 < r; n2++) x[c * r + n2] = buf[swz<T>(pos<S>(t, c, n2))];
+            for (int n2 = 0; n2 < r; n2++) x[c * r + n2] = Exch<T, M>::get(buf, pos<S>(t, c, n2));
     }
 
     template <int S, bool INV>
@@ -270,7 +293,7 @@ struct TeamFft {
     }
 
     template <int S>
-    __device__ static __forceinline__ void forward_from(cplx<T> *x, cplx<T> *buf, const cplx<T> *tw, int t, int bar_id) {
+    __device__ static __forceinline__ void forward_from(cplx<T> *x, void *buf, const cplx<T> *tw, int t, int bar_id) {
         constexpr int r = Stage<M, S>::r;
 #pragma unroll
         for (int c = 0; c < R / r; c++) dft<T, false, r>(x + c * r);
@@ -285,7 +308,7 @@ struct TeamFft {
     }
 
     template <int S>
-    __device__ static __forceinline__ void inverse_from(cplx<T> *x, cplx<T> *buf, const cplx<T> *tw, int t, int bar_id) {
+    __device__ static __forceinline__ void inverse_from(cplx<T> *x, void *buf, const cplx<T> *tw, int t, int bar_id) {
         constexpr int r = Stage<M, S>::r;
         twiddle<S, true>(x, tw, t);
 #pragma unroll
@@ -301,12 +324,12 @@ struct TeamFft {
 
     // Folded negacyclic transform.  In: x[n2] = a_j - i a_{j+M} for j = t + NT*n2 (no twist applied).
     // Out: the M evaluation points in slot order.
-    __device__ static __forceinline__ void forward(cplx<T> *x, cplx<T> *buf, const cplx<T> *tw, int t, int bar_id) {
+    __device__ static __forceinline__ void forward(cplx<T> *x, void *buf, const cplx<T> *tw, int t, int bar_id) {
         fold_consts<false>(x);
         forward_from<0>(x, buf, tw, t, bar_id);
     }
     // Slot order in -> x[n2] = M * (c_j - i c_{j+M}), j = t + NT*n2 (twist removed).
-    __device__ static __forceinline__ void inverse(cplx<T> *x, cplx<T> *buf, const cplx<T> *tw, int t, int bar_id) {
+    __device__ static __forceinline__ void inverse(cplx<T> *x, void *buf, const cplx<T> *tw, int t, int bar_id) {
         inverse_from<NS - 1>(x, buf, tw, t, bar_id);
         fold_consts<true>(x);
     }
