@@ -196,26 +196,33 @@ struct Exch;
 template <int M>
 struct Exch<double, M> {
     static constexpr int bytes = 16 * (M + (M >> 3));
-    __device__ static __forceinline__ void put(void *buf, int p, cplx<double> v) {
-        reinterpret_cast<cplx<double> *>(buf)[p + (p >> 3)] = v;
+    // element index of position p; every stage pattern is affine in it: idx(base + d) = idx(base) + delta
+    __host__ __device__ static constexpr int index(int p) { return p + (p >> 3); }
+    __host__ __device__ static constexpr int delta(int p, int p0) { return index(p) - index(p0); }
+    __device__ static __forceinline__ int combine(int base, int d) { return base + d; }
+    __device__ static __forceinline__ void put(void *buf, int i, cplx<double> v) {
+        reinterpret_cast<cplx<double> *>(buf)[i] = v;
     }
-    __device__ static __forceinline__ cplx<double> get(const void *buf, int p) {
-        return reinterpret_cast<const cplx<double> *>(buf)[p + (p >> 3)];
+    __device__ static __forceinline__ cplx<double> get(const void *buf, int i) {
+        return reinterpret_cast<const cplx<double> *>(buf)[i];
     }
 };
 template <int M>
 struct Exch<float, M> {
     static constexpr int bytes = 8 * M;
-    __device__ static __forceinline__ void put(void *buf, int p, cplx<float> v) {
+    // XOR swizzle; every stage pattern is XOR-separable: idx(pos(t,c,n2)) = idx(pos(t,0,0)) ^ delta(c,n2)
+    // (checked for the 8*8*4, 8*8*8 and 8*8*8*2 plans), so each access costs one XOR with a constant
+    __host__ __device__ static constexpr int index(int p) { return p ^ ((p >> 3) & 31); }
+    __host__ __device__ static constexpr int delta(int p, int p0) { return index(p) ^ index(p0); }
+    __device__ static __forceinline__ int combine(int base, int d) { return base ^ d; }
+    __device__ static __forceinline__ void put(void *buf, int i, cplx<float> v) {
         float *re = reinterpret_cast<float *>(buf);
-        const int q = p ^ ((p >> 3) & 31);
-        re[q] = v.re;
-        re[M + q] = v.im;
+        re[i] = v.re;
+        re[M + i] = v.im;
     }
-    __device__ static __forceinline__ cplx<float> get(const void *buf, int p) {
+    __device__ static __forceinline__ cplx<float> get(const void *buf, int i) {
         const float *re = reinterpret_cast<const float *>(buf);
-        const int q = p ^ ((p >> 3) & 31);
-        return {re[q], re[M + q]};
+        return {re[i], re[M + i]};
     }
 };
 
@@ -233,29 +240,38 @@ struct TeamFft {
 
     // position of register (c, n2) of thread t at stage S
     template <int S>
-    __device__ static __forceinline__ int pos(int t, int c, int n2) {
+    __host__ __device__ static constexpr int pos(int t, int c, int n2) {
         constexpr int L = Stage<M, S>::L, st = Stage<M, S>::stride;
         const int b = t + NT * c;
         const int q = b / st, n1 = b - q * st;
         return q * L + n1 + st * n2;
     }
+    // compile-time part of the exchange index of register (c, n2) at stage S
+    template <int S>
+    __host__ __device__ static constexpr int delta(int c, int n2) {
+        return Exch<T, M>::delta(pos<S>(0, c, n2), pos<S>(0, 0, 0));
+    }
 
     template <int S>
     __device__ static __forceinline__ void store(const cplx<T> *x, void *buf, int t) {
         constexpr int r = Stage<M, S>::r;
+        const int base = Exch<T, M>::index(pos<S>(t, 0, 0));
 #pragma unroll
         for (int c = 0; c < R / r; c++)
 #pragma unroll
-            for (int n2 = 0; n2 < r; n2++) Exch<T, M>::put(buf, pos<S>(t, c, n2), x[c * r + n2]);
+            for (int n2 = 0; n2 < r; n2++)
+                Exch<T, M>::put(buf, Exch<T, M>::combine(base, delta<S>(c, n2)), x[c * r + n2]);
     }
 
     template <int S>
     __device__ static __forceinline__ void load(cplx<T> *x, const void *buf, int t) {
         constexpr int r = Stage<M, S>::r;
+        const int base = Exch<T, M>::index(pos<S>(t, 0, 0));
 #pragma unroll
         for (int c = 0; c < R / r; c++)
 #pragma unroll
-            for (int n2 = 0; n2 < r; n2++) x[c * r + n2] = Exch<T, M>::get(buf, pos<S>(t, c, n2));
+            for (int n2 = 0; n2 < r; n2++)
+                x[c * r + n2] = Exch<T, M>::get(buf, Exch<T, M>::combine(base, delta<S>(c, n2)));
     }
 
     template <int S, bool INV>
