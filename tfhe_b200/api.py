@@ -75,6 +75,7 @@ def lib():
         L.tfheb_br_variants.argtypes = [_I32, _I32, _V, _V, _I32, _V]
         L.tfheb_set_br_variant.argtypes = [_V, _I32, _I32]
         L.tfheb_autotune.argtypes = [_V, _I32, _I32, _V, _I32]
+        L.tfheb_set_keyswitch_kernel.argtypes = [_V, _I32]
         _lib = L
     return _lib
 
@@ -223,6 +224,10 @@ class CloudKey:
 
     def set_br_variant(self, precision, variant):
         _check(lib().tfheb_set_br_variant(self.h, precision, variant), "tfheb_set_br_variant")
+
+    def set_keyswitch_kernel(self, which):
+        """0 = default, 1 = one CTA per sample, 2 = tiled (bit-identical results)."""
+        _check(lib().tfheb_set_keyswitch_kernel(self.h, which), "tfheb_set_keyswitch_kernel")
 
     def set_wait_timeout(self, seconds):
         _check(lib().tfheb_set_wait_timeout(self.h, ctypes.c_uint64(int(seconds * 1e9))), "tfheb_set_wait_timeout")

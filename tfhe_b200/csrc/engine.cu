@@ -170,7 +170,7 @@ static tfheb_status run_pipeline(CloudKey &ck, int precision, int count, int boo
     }));
     TFHEB_CUDA(timed(ck, 2, s, [&] { return launch_extract(p, ck.d_gdesc, count, ck.d_acc, ck.d_ksin, kN1, s); }));
     TFHEB_CUDA(timed(ck, 3, s, [&] {
-        return launch_keyswitch(p, ck.d_ksk, ck.ks_stride, count, ck.d_ksin, kN1, d_out, s);
+        return launch_keyswitch(ck, count, ck.d_ksin, kN1, d_out, s);
     }));
     g_launches += 4;
     ck.launches += 4;
@@ -300,7 +300,7 @@ void tfheb_cloud_key_free(tfheb_cloud_key *c) {
             cudaFree(d.bsk);
             cudaFree(d.tables);
         }
-        cudaFree(ck.d_ksk);
+        free_keyswitch_key(ck.dksk);
         cudaFree(ck.d_bara);
         cudaFree(ck.d_acc);
         cudaFree(ck.d_ksin);
@@ -358,16 +358,8 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32
         TFHEB_CUDA(cudaMemset(ck.d_err, 0, sizeof(int32_t)));
     }
     const tfheb_params &p = ck.p;
-    // keyswitching key, rows padded to a multiple of 4 int32 (16-byte aligned vector loads)
-    if (!ck.d_ksk) {
-        ck.ks_stride = (p.n + 1 + 3) & ~3;
-        const size_t rows = (size_t)p.k * p.N * p.ks_t * (1 << p.ks_basebit);
-        std::vector<int32_t> padded(rows * ck.ks_stride, 0);
-        for (size_t r = 0; r < rows; r++)
-            std::memcpy(&padded[r * ck.ks_stride], &ck.ksk[r * (p.n + 1)], (p.n + 1) * 4);
-        TFHEB_CUDA(cudaMalloc((void **)&ck.d_ksk, padded.size() * 4));
-        TFHEB_CUDA(cudaMemcpy(ck.d_ksk, padded.data(), padded.size() * 4, cudaMemcpyHostToDevice));
-    }
+    // keyswitching key in the layouts of both keyswitch kernels
+    TFHEB_CUDA(upload_keyswitch_key(ck));
     std::vector<double> tab;
     build_tables_fp64(p.N, tab);
     for (int prec = 0; prec < 2; prec++) {
@@ -544,11 +536,11 @@ tfheb_status tfheb_keyswitch_device(tfheb_cloud_key *c, int32_t count, const int
     if (!c || count < 0 || !d_in || !d_out) return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
     CloudKey &ck = c->ck;
-    if (ck.device < 0 || !ck.d_ksk) return TFHEB_ERR_INVALID;
+    if (ck.device < 0 || !ck.dksk.rows) return TFHEB_ERR_INVALID;
     TFHEB_CUDA(cudaSetDevice(ck.device));
     if (count == 0) return TFHEB_OK;
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
-    TFHEB_CUDA(launch_keyswitch(ck.p, ck.d_ksk, ck.ks_stride, count, d_in, ck.p.k * ck.p.N + 1, d_out, s));
+    TFHEB_CUDA(launch_keyswitch(ck, count, d_in, ck.p.k * ck.p.N + 1, d_out, s));
     g_launches += 1;
     return TFHEB_OK;
 }
@@ -583,6 +575,18 @@ tfheb_status tfheb_set_br_variant(tfheb_cloud_key *c, int32_t precision, int32_t
     if (variant < 0 || variant >= br_variants(c->ck.p.N, precision, nullptr, nullptr, 0)) return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
     c->ck.br_variant[precision] = variant;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_set_keyswitch_kernel(tfheb_cloud_key *c, int32_t which) {
+    if (!c || which < 0 || which > 2) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    const tfheb_params &p = c->ck.p;
+    if (which == 2 && !(p.ks_t == 8 && p.ks_basebit == 2)) {
+        set_error("tfheb_set_keyswitch_kernel: no tiled keyswitch for this parameter set");
+        return TFHEB_ERR_UNSUPPORTED;
+    }
+    c->ck.ks_kernel = which;
     return TFHEB_OK;
 }
 

@@ -39,6 +39,16 @@ struct DeviceBsk {
     int split_shift = 0;      // split mode: weight of the high limb is 2^split_shift
 };
 
+// Device-side keyswitching key in the two layouts of the two keyswitch kernels (keyswitch.cu).
+struct DeviceKsk {
+    int32_t *rows = nullptr;   // per-gate kernel: [kN][t][base][stride], rows zero padded
+    int stride = 0;            // padded row length (multiple of 4 >= n+1)
+    int32_t *tiles = nullptr;  // tiled kernel: [slice][kN][t][base-1][tile_rs] (h = 0 rows dropped)
+    int tile_cw = 0;           // output columns per warp of the tiled kernel (0: tiled kernel unavailable)
+    int tile_slices = 0;       // column slices of 4 * tile_cw columns covering n+1
+    int tile_slots = 0;        // resident CTAs of the tiled kernel on the device
+};
+
 struct CloudKey {
     tfheb_params p{};
     std::vector<int32_t> bsk_coef;  // [n][kpl][k+1][N] coefficient domain (host)
@@ -46,8 +56,8 @@ struct CloudKey {
     // device state
     int device = -1;
     DeviceBsk dbsk[2];              // [TFHEB_FP64], [TFHEB_SPLIT_FP32]
-    int32_t *d_ksk = nullptr;       // [kN][t][base][ks_stride]
-    int ks_stride = 0;              // padded row length (multiple of 4 >= n+1)
+    DeviceKsk dksk;
+    int ks_kernel = 0;              // 0 = choose by batch size, 1 = per-gate, 2 = tiled
     cudaStream_t stream = nullptr;
     // scratch (grown on demand)
     int32_t *d_bara = nullptr;
@@ -111,8 +121,12 @@ cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const Devi
 int br_variants(int N, int precision, int *G, int *D, int cap);
 cudaError_t launch_extract(const tfheb_params &p, const GateDesc *d_desc, int count, const int32_t *acc,
                            int32_t *out, int out_stride, cudaStream_t s);
-cudaError_t launch_keyswitch(const tfheb_params &p, const int32_t *d_ksk, int ks_stride, int count,
-                             const int32_t *in, int in_stride, int32_t *out, cudaStream_t s);
+// keyswitch.cu: device key upload (both layouts) and the keyswitch of `count` extracted samples
+// (rows of in_stride int32) into rows of n+1 int32.
+cudaError_t upload_keyswitch_key(CloudKey &ck);
+void free_keyswitch_key(DeviceKsk &d);
+cudaError_t launch_keyswitch(const CloudKey &ck, int count, const int32_t *in, int in_stride, int32_t *out,
+                             cudaStream_t s);
 int blind_rotate_supported(const tfheb_params &p);
 cudaError_t launch_negate(const int32_t *in, int32_t *out, size_t count, cudaStream_t s);
 

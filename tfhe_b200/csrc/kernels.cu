@@ -5,7 +5,7 @@
 //   (the blind rotation itself lives in blind_rotate.cu)
 //   extract_kernel       sample extraction at index 0, MUX recombination   (lwe.cpp:41-60,
 //                        boot-gates.cpp:360-364)
-//   keyswitch_kernel     integer gather-accumulate keyswitch               (lwe-keyswitch-functions.cpp:114-238)
+//   (the keyswitch kernels live in keyswitch.cu)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -100,68 +100,6 @@ cudaError_t launch_negate(const int32_t *in, int32_t *out, size_t count, cudaStr
     const int blocks = (int)std::min<size_t>((count + 255) / 256, 148 * 8);
     negate_kernel<<<blocks, 256, 0, s>>>(reinterpret_cast<const uint32_t *>(in), reinterpret_cast<uint32_t *>(out),
                                          count);
-    return cudaGetLastError();
-}
-
-// ============================================================================================
-// keyswitch
-// ============================================================================================
-
-// One CTA per gate; thread owns 4 consecutive output coefficients (int4 loads of the key rows).
-// ksk rows: [kN][t][base][ks_stride], ks_stride a multiple of 4, zero padded.
-__global__ void __launch_bounds__(256) keyswitch_kernel(const int32_t *__restrict__ ksk, int ks_stride,
-                                                        const uint32_t *__restrict__ in, int in_stride,
-                                                        uint32_t *__restrict__ out, int n, int kN, int t,
-                                                        int basebit) {
-    const int g = blockIdx.x;
-    const uint32_t *x = in + (size_t)g * in_stride;
-    const int c4 = threadIdx.x * 4;
-    const bool active = c4 < ks_stride;
-    const int base = 1 << basebit;
-    const uint32_t mask = (uint32_t)base - 1;
-    const uint32_t prec_offset = 1u << (32 - (1 + basebit * t));  // lwe-keyswitch-functions.cpp:119
-    uint32_t acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
-    extern __shared__ uint32_t s_a[];  // the input mask, kN values
-    for (int i = threadIdx.x; i < kN; i += blockDim.x) s_a[i] = x[i] + prec_offset;
-    __syncthreads();
-    if (active) {
-        const size_t row_i = (size_t)t * base * ks_stride;
-        for (int i = 0; i < kN; i++) {
-            const uint32_t aibar = s_a[i];
-            const int4 *rows = reinterpret_cast<const int4 *>(ksk + (size_t)i * row_i) + (c4 >> 2);
-            for (int j = 0; j < t; j++) {
-                const uint32_t aij = (aibar >> (32 - (j + 1) * basebit)) & mask;
-                if (aij != 0) {
-                    const int4 v = __ldg(rows + ((size_t)(j * base + aij) * ks_stride >> 2));
-                    acc0 -= (uint32_t)v.x;
-                    acc1 -= (uint32_t)v.y;
-                    acc2 -= (uint32_t)v.z;
-                    acc3 -= (uint32_t)v.w;
-                }
-            }
-        }
-        // result = (0, b) - sum  (lwe-keyswitch-functions.cpp:233-237)
-        uint32_t *o = out + (size_t)g * (n + 1);
-        const uint32_t b = x[kN];
-        const uint32_t accs[4] = {acc0, acc1, acc2, acc3};
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int col = c4 + e;
-            if (col < n) o[col] = accs[e];
-            else if (col == n) o[col] = b + accs[e];
-        }
-    }
-}
-
-cudaError_t launch_keyswitch(const tfheb_params &p, const int32_t *d_ksk, int ks_stride, int count,
-                             const int32_t *in, int in_stride, int32_t *out, cudaStream_t s) {
-    if (count <= 0) return cudaSuccess;
-    const int kN = p.k * p.N;
-    const int threads = ((ks_stride / 4 + 31) / 32) * 32;
-    if (threads > 256) return cudaErrorInvalidValue;
-    keyswitch_kernel<<<count, threads, sizeof(uint32_t) * kN, s>>>(
-        d_ksk, ks_stride, reinterpret_cast<const uint32_t *>(in), in_stride, reinterpret_cast<uint32_t *>(out), p.n,
-        kN, p.ks_t, p.ks_basebit);
     return cudaGetLastError();
 }
 

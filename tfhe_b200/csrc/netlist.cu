@@ -130,7 +130,7 @@ cudaError_t enqueue_netlist(tfheb_netlist *nl, CloudKey &ck, int precision, int3
             if (e != cudaSuccess) break;
             e = launch_extract(p, nl->d_gate + L.gate_off, L.gates, nl->d_acc, nl->d_ksin, kN1, s);
             if (e != cudaSuccess) break;
-            e = launch_keyswitch(p, ck.d_ksk, ck.ks_stride, L.gates, nl->d_ksin, kN1,
+            e = launch_keyswitch(ck, L.gates, nl->d_ksin, kN1,
                                  nl->d_wires + (size_t)L.out_row * n1, s);
             launches += 4;
         }

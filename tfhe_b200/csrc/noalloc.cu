@@ -138,7 +138,7 @@ extern "C" tfheb_status tfheb_gate_batch_device_noalloc(tfheb_cloud_key *c, int3
                                 nullptr, acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns,
                                 ck.br_variant[precision]);
     if (e == cudaSuccess) e = launch_extract(p, gd, count, acc, ksin, kN1, s);
-    if (e == cudaSuccess) e = launch_keyswitch(p, ck.d_ksk, ck.ks_stride, count, ksin, kN1, d_out, s);
+    if (e == cudaSuccess) e = launch_keyswitch(ck, count, ksin, kN1, d_out, s);
     if (e != cudaSuccess) {
         set_error(std::string("tfheb_gate_batch_device_noalloc: ") + cudaGetErrorString(e));
         return TFHEB_ERR_CUDA;
