@@ -33,9 +33,10 @@ namespace tfheb {
 
 // ---- exact conversions without the conversion (XU) pipe ------------------------------------
 
-// small integer v (|v| < 2^22) -> float, via the 1.5*2^23 bias
-__device__ __forceinline__ float biased_to_float(uint32_t biased_bits_minus_magic, float bias) {
-    return __int_as_float(0x4B400000 + (int32_t)biased_bits_minus_magic) - bias;
+// small non-negative integer d (d < 2^22) -> float d - (bias - 1.5*2^23): the bits of 1.5*2^23 + d are
+// 0x4B400000 | d, so the digit mask and this OR fuse into one logic op
+__device__ __forceinline__ float biased_to_float(uint32_t d, float bias) {
+    return __int_as_float(0x4B400000u | d) - bias;
 }
 // round-to-nearest of a float with |v| < 2^44, reduced mod 2^32 (FMA/ALU ops only)
 __device__ __forceinline__ uint32_t round_f32_mod32(float v) {
@@ -138,8 +139,11 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     cplx<T> *s_tab = reinterpret_cast<cplx<T> *>(smem + Lay::tables);
-    const cplx<T> *g_tab = reinterpret_cast<const cplx<T> *>(args.tables);
-    for (int i = tid; i < Lay::TW; i += blockDim.x) s_tab[i] = g_tab[i];
+    {
+        const int4 *g_tab = reinterpret_cast<const int4 *>(args.tables);
+        int4 *s_tab4 = reinterpret_cast<int4 *>(smem + Lay::tables);
+        for (int i = tid; i < (int)(Lay::tables_bytes / 16); i += blockDim.x) s_tab4[i] = g_tab[i];
+    }
     __syncthreads();
 
     const int total_chunks = args.nsteps * KPL;
@@ -213,15 +217,24 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
     int c = 0;  // key-row (chunk) counter, same sequence as the producer
     for (int step = 0; step < args.nsteps; step++) {
         const int ai = s_bara[step] & (2 * N - 1);
-        cplx<T> acc_hi[KP1][kR];
-        cplx<T> acc_lo[SPLIT ? KP1 : 1][kR];
+        // FP64: one accumulator spectrum per output polynomial.  Split: hi- and lo-limb spectra as
+        // packed register pairs over the slots (2m, 2m+1).
+        cplx<T> acc_hi[SPLIT ? 1 : KP1][kR];
+        cpair acc_h[SPLIT ? KP1 : 1][kR / 2], acc_l[SPLIT ? KP1 : 1][kR / 2];
+        if constexpr (SPLIT) {
 #pragma unroll
-        for (int v = 0; v < KP1; v++)
+            for (int v = 0; v < KP1; v++)
 #pragma unroll
-            for (int r = 0; r < kR; r++) {
-                acc_hi[v][r] = {T(0), T(0)};
-                if (SPLIT) acc_lo[SPLIT ? v : 0][r] = {T(0), T(0)};
-            }
+                for (int m = 0; m < kR / 2; m++) {
+                    acc_h[v][m] = {{0.f, 0.f}, {0.f, 0.f}};
+                    acc_l[v][m] = {{0.f, 0.f}, {0.f, 0.f}};
+                }
+        } else {
+#pragma unroll
+            for (int v = 0; v < KP1; v++)
+#pragma unroll
+                for (int r = 0; r < kR; r++) acc_hi[v][r] = {T(0), T(0)};
+        }
 
 #pragma unroll 1
         for (int u = 0; u < KP1; u++) {
@@ -248,20 +261,30 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                 const int s = c % D;
                 wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns, args.err);
                 const unsigned char *stage = smem + Lay::ring + (size_t)s * Lay::chunk;
+                if constexpr (SPLIT) {
+                    // key row: [v][m][limb][t] x float4 {re(2m), re(2m+1), im(2m), im(2m+1)}
 #pragma unroll
-                for (int v = 0; v < KP1; v++)
+                    for (int m = 0; m < kR / 2; m++) {
+                        const cpair zp = make_cpair(z[2 * m], z[2 * m + 1]);
+                        const float2 nzi = mul2(zp.im, make_float2(-1.f, -1.f));
 #pragma unroll
-                    for (int r = 0; r < kR; r++) {
-                        const size_t off = ((size_t)(v * kR + r) * NT + t) * 16;
-                        if constexpr (SPLIT) {
-                            const float4 b = *reinterpret_cast<const float4 *>(stage + off);
-                            cmac(acc_hi[v][r], z[r], cplx<T>{b.x, b.y});
-                            cmac(acc_lo[SPLIT ? v : 0][r], z[r], cplx<T>{b.z, b.w});
-                        } else {
+                        for (int v = 0; v < KP1; v++) {
+                            const float4 *kp = reinterpret_cast<const float4 *>(
+                                stage + ((size_t)((v * (kR / 2) + m) * 2) * NT + t) * 16);
+                            cmac_pair(acc_h[v][m], zp, nzi, kp[0]);
+                            cmac_pair(acc_l[v][m], zp, nzi, kp[NT]);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int v = 0; v < KP1; v++)
+#pragma unroll
+                        for (int r = 0; r < kR; r++) {
+                            const size_t off = ((size_t)(v * kR + r) * NT + t) * 16;
                             const double2 b = *reinterpret_cast<const double2 *>(stage + off);
                             cmac(acc_hi[v][r], z[r], cplx<T>{(T)b.x, (T)b.y});
                         }
-                    }
+                }
                 mbar_arrive(empty_bar(s));
             }
         }
@@ -272,8 +295,16 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
             uint32_t c0[kR], c1[kR];
             {
                 cplx<T> z[kR];
+                if constexpr (SPLIT) {
 #pragma unroll
-                for (int r = 0; r < kR; r++) z[r] = acc_hi[v][r];
+                    for (int m = 0; m < kR / 2; m++) {
+                        z[2 * m] = {acc_h[v][m].re.x, acc_h[v][m].im.x};
+                        z[2 * m + 1] = {acc_h[v][m].re.y, acc_h[v][m].im.y};
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < kR; r++) z[r] = acc_hi[v][r];
+                }
                 F::inverse(z, buf, s_tw, t, bar_id);
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
@@ -290,7 +321,10 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
             if constexpr (SPLIT) {
                 cplx<T> z[kR];
 #pragma unroll
-                for (int r = 0; r < kR; r++) z[r] = acc_lo[SPLIT ? v : 0][r];
+                for (int m = 0; m < kR / 2; m++) {
+                    z[2 * m] = {acc_l[v][m].re.x, acc_l[v][m].im.x};
+                    z[2 * m + 1] = {acc_l[v][m].re.y, acc_l[v][m].im.y};
+                }
                 F::inverse(z, buf, s_tw, t, bar_id);
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
@@ -342,10 +376,14 @@ struct BrVariant {
 };
 static const BrVariant kBrVariants[] = {
     {1024, TFHEB_SPLIT_FP32, 7, 4, launch_g<float, 1024, true, 7, 4>},
+    {1024, TFHEB_SPLIT_FP32, 7, 6, launch_g<float, 1024, true, 7, 6>},
+    {1024, TFHEB_SPLIT_FP32, 6, 4, launch_g<float, 1024, true, 6, 4>},
+    {1024, TFHEB_SPLIT_FP32, 6, 6, launch_g<float, 1024, true, 6, 6>},
     {1024, TFHEB_SPLIT_FP32, 5, 4, launch_g<float, 1024, true, 5, 4>},
     {1024, TFHEB_SPLIT_FP32, 4, 4, launch_g<float, 1024, true, 4, 4>},
     {1024, TFHEB_FP64, 3, 4, launch_g<double, 1024, false, 3, 4>},
     {1024, TFHEB_FP64, 4, 4, launch_g<double, 1024, false, 4, 4>},
+    {1024, TFHEB_FP64, 4, 6, launch_g<double, 1024, false, 4, 6>},
     {1024, TFHEB_FP64, 2, 4, launch_g<double, 1024, false, 2, 4>},
     {2048, TFHEB_SPLIT_FP32, 3, 3, launch_g<float, 2048, true, 3, 3>},
     {2048, TFHEB_SPLIT_FP32, 2, 3, launch_g<float, 2048, true, 2, 3>},

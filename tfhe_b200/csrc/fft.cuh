@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+
 namespace tfheb {
 
 template <typename T>
@@ -116,6 +117,32 @@ __device__ __forceinline__ void dft(cplx<T> *x) {
     if constexpr (RADIX == 8) dft8<T, INV>(x);
     else if constexpr (RADIX == 4) dft4<T, INV>(x);
     else dft2<T, INV>(x);
+}
+
+// ---- packed FP32 (sm_100 f32x2): two complex numbers per register pair ------------------------
+// A "cpair" holds two complex numbers in planar form, re = {a.re, b.re}, im = {a.im, b.im}.  Each
+// packed instruction performs the two correctly rounded scalar operations, so packed code gives bit
+// for bit the results of the scalar code with half the issued FP32 instructions.  The blind
+// rotation uses it for the multiply-accumulate against the key; packing the FFT codelets as well
+// measured slower (register-pair moves and longer dependency chains outweigh the saved issues).
+
+struct cpair {
+    float2 re, im;
+};
+
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+__device__ __forceinline__ cpair make_cpair(cplx<float> a, cplx<float> b) { return {{a.re, b.re}, {a.im, b.im}}; }
+
+// acc += z * k on a register pair, with the scalar cmac operation order; nzi = -z.im, k = float4
+// {re, re', im, im'}
+__device__ __forceinline__ void cmac_pair(cpair &acc, const cpair &z, float2 nzi, float4 k) {
+    const float2 kr{k.x, k.y}, ki{k.z, k.w};
+    acc.re = fma2(z.re, kr, acc.re);
+    acc.re = fma2(nzi, ki, acc.re);
+    acc.im = fma2(z.re, ki, acc.im);
+    acc.im = fma2(z.im, kr, acc.im);
 }
 
 // ---- plans -----------------------------------------------------------------------------------

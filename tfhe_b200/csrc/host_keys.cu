@@ -291,7 +291,8 @@ void build_tables_fp64(int N, std::vector<double> &tab) {
 }
 
 // bsk_coef [n][kpl][k+1][N] -> FFT domain, slot layout [n][kpl][k+1][R][NT], 16 bytes per slot:
-//   FP64: double2 (re, im) of B_k / M;   split FP32: float4 (hi.re, hi.im, lo.re, lo.im) / M
+//   FP64: double2 (re, im) of B_k / M at [R][NT];
+//   split FP32: per register pair (2m, 2m+1) and limb, float4 {re, re', im, im'} of B_k / M at [4][2][NT]
 void transform_bsk(const tfheb_params &p, const int32_t *bsk_coef, int precision, int split_shift,
                    std::vector<uint8_t> &out) {
     const int N = p.N, M = N / 2, NT = M / kR, kpl = (p.k + 1) * p.l;
@@ -334,14 +335,20 @@ void transform_bsk(const tfheb_params &p, const int32_t *bsk_coef, int precision
                 }
                 fold_fft(hi.data(), zh);
                 fold_fft(lo.data(), zl);
+                // [m < 4][limb: hi, lo][t] x float4 {re(r), re(r+1), im(r), im(r+1)}, r = 2m: the
+                // register pairs of the packed multiply-accumulate
                 float *d = reinterpret_cast<float *>(dst);
-                for (int s = 0; s < kR * NT; s++) {
-                    const cd h = zh[sf[s]] * scale, l = zl[sf[s]] * scale;
-                    d[4 * s] = (float)h.real();
-                    d[4 * s + 1] = (float)h.imag();
-                    d[4 * s + 2] = (float)l.real();
-                    d[4 * s + 3] = (float)l.imag();
-                }
+                for (int r = 0; r < kR; r++)
+                    for (int t = 0; t < NT; t++) {
+                        const int s = r * NT + t, m = r >> 1, odd = r & 1;
+                        const cd h = zh[sf[s]] * scale, l = zl[sf[s]] * scale;
+                        float *eh = d + ((size_t)(m * 2 + 0) * NT + t) * 4;
+                        float *el = d + ((size_t)(m * 2 + 1) * NT + t) * 4;
+                        eh[odd] = (float)h.real();
+                        eh[2 + odd] = (float)h.imag();
+                        el[odd] = (float)l.real();
+                        el[2 + odd] = (float)l.imag();
+                    }
             }
         }
     });
