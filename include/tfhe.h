@@ -20,6 +20,7 @@
 #define TFHE_B200_DROPIN_TFHE_H
 
 #include <stdint.h>
+#include <stdio.h>
 
 #ifdef __cplusplus
 #define TFHE_B200_EXPORT extern "C"
@@ -152,6 +153,24 @@ TFHE_B200_EXPORT void bootsNAND_batch(LweSample *results, const LweSample *a, co
                                       const TFheGateBootstrappingCloudKeySet *bk);
 TFHE_B200_EXPORT void bootsMUX_batch(LweSample *results, const LweSample *a, const LweSample *b, const LweSample *c,
                                      int32_t count, const TFheGateBootstrappingCloudKeySet *bk);
+
+/* ---- tfhe_io.h: files in the reference's format (tfhe_io.cpp:90-136, 1010-1220) -------------
+ * Same layout byte for byte, so key sets and ciphertexts move between this library and tfhe. */
+TFHE_B200_EXPORT void export_lweSample_toFile(FILE *F, const LweSample *lwesample, const LweParams *params);
+TFHE_B200_EXPORT void import_lweSample_fromFile(FILE *F, LweSample *lwesample, const LweParams *params);
+TFHE_B200_EXPORT void export_gate_bootstrapping_ciphertext_toFile(FILE *F, const LweSample *sample,
+                                                                  const TFheGateBootstrappingParameterSet *params);
+TFHE_B200_EXPORT void import_gate_bootstrapping_ciphertext_fromFile(FILE *F, LweSample *sample,
+                                                                    const TFheGateBootstrappingParameterSet *params);
+TFHE_B200_EXPORT void export_tfheGateBootstrappingParameterSet_toFile(FILE *F,
+                                                                      const TFheGateBootstrappingParameterSet *params);
+TFHE_B200_EXPORT TFheGateBootstrappingParameterSet *new_tfheGateBootstrappingParameterSet_fromFile(FILE *F);
+TFHE_B200_EXPORT void export_tfheGateBootstrappingCloudKeySet_toFile(FILE *F,
+                                                                     const TFheGateBootstrappingCloudKeySet *keyset);
+TFHE_B200_EXPORT TFheGateBootstrappingCloudKeySet *new_tfheGateBootstrappingCloudKeySet_fromFile(FILE *F);
+TFHE_B200_EXPORT void export_tfheGateBootstrappingSecretKeySet_toFile(FILE *F,
+                                                                      const TFheGateBootstrappingSecretKeySet *keyset);
+TFHE_B200_EXPORT TFheGateBootstrappingSecretKeySet *new_tfheGateBootstrappingSecretKeySet_fromFile(FILE *F);
 
 /* 0 = FP64 (default), 1 = split FP32.  Applies to subsequent gate calls of this process. */
 TFHE_B200_EXPORT void tfhe_b200_set_precision(int32_t precision);

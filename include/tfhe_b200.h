@@ -89,6 +89,30 @@ tfheb_status tfheb_secret_key_import(const tfheb_params *p, const int32_t *lwe_k
 tfheb_status tfheb_secret_key_export(const tfheb_secret_key *sk, int32_t *lwe_key, int32_t *tlwe_key);
 tfheb_status tfheb_cloud_key_export(const tfheb_cloud_key *ck, int32_t *bsk, int32_t *ksk);
 tfheb_status tfheb_cloud_key_params(const tfheb_cloud_key *ck, tfheb_params *out);
+
+/* Files in the reference's format (tfhe_io.cpp): what one side writes, the other reads.
+ *   tfheb_params_save / _load          export_tfheGateBootstrappingParameterSet_toFile /
+ *                                      new_tfheGateBootstrappingParameterSet_fromFile (:1036-1049)
+ *   tfheb_cloud_key_save / _load       export_ / new_tfheGateBootstrappingCloudKeySet_..File (:1125-1136)
+ *   tfheb_secret_keyset_save / _load   export_ / new_tfheGateBootstrappingSecretKeySet_..File (:1179-1190)
+ *   tfheb_ciphertexts_save / _load     export_gate_bootstrapping_ciphertext_toFile /
+ *                                      import_gate_bootstrapping_ciphertext_fromFile (:1211-1220),
+ *                                      `count` samples back to back, [count][n+1] int32; variances
+ *                                      may be NULL (saved as 0, not returned).
+ * A parameter file stores reals with 8 decimals ("%.8lf"), so a loaded ks_stdev / bk_stdev is the
+ * rounded value, as in the reference.  Loading checks section titles and block type ids and
+ * returns TFHEB_ERR_INVALID (with tfheb_last_error) where the reference aborts. */
+tfheb_status tfheb_params_save(const char *path, const tfheb_params *p);
+tfheb_status tfheb_params_load(const char *path, tfheb_params *p);
+tfheb_status tfheb_cloud_key_save(const tfheb_cloud_key *ck, const char *path);
+tfheb_status tfheb_cloud_key_load(const char *path, tfheb_cloud_key **ck);
+tfheb_status tfheb_secret_keyset_save(const tfheb_secret_key *sk, const tfheb_cloud_key *ck, const char *path);
+tfheb_status tfheb_secret_keyset_load(const char *path, tfheb_secret_key **sk, tfheb_cloud_key **ck);
+tfheb_status tfheb_ciphertexts_save(const char *path, const tfheb_params *p, int32_t count, const int32_t *cts,
+                                    const double *variances);
+tfheb_status tfheb_ciphertexts_load(const char *path, const tfheb_params *p, int32_t count, int32_t *cts,
+                                    double *variances);
+
 /* Replaces delete_gate_bootstrapping_{secret,cloud}_keyset (tfhe_gate_bootstrapping.cpp:111-130). */
 void tfheb_secret_key_free(tfheb_secret_key *sk);
 void tfheb_cloud_key_free(tfheb_cloud_key *ck);

@@ -341,3 +341,71 @@ void rs_extern_mul(void *h, int32_t i, int32_t *acc) {
     delete_TLweSample(x);
 }
 }
+
+// ---- the reference's own file format (tfhe_io.cpp), through its FILE* functions -------------
+extern "C" {
+
+int rs_save_params(void *h, const char *path) {
+    FILE *F = std::fopen(path, "wb");
+    if (!F) return -1;
+    export_tfheGateBootstrappingParameterSet_toFile(F, static_cast<RsKeys *>(h)->params);
+    return std::fclose(F);
+}
+
+int rs_save_secret_keyset(void *h, const char *path) {
+    FILE *F = std::fopen(path, "wb");
+    if (!F) return -1;
+    export_tfheGateBootstrappingSecretKeySet_toFile(F, static_cast<RsKeys *>(h)->sk);
+    return std::fclose(F);
+}
+
+int rs_save_cloud_keyset(void *h, const char *path) {
+    FILE *F = std::fopen(path, "wb");
+    if (!F) return -1;
+    export_tfheGateBootstrappingCloudKeySet_toFile(F, &static_cast<RsKeys *>(h)->sk->cloud);
+    return std::fclose(F);
+}
+
+// count ciphertexts [count][n+1] with the given variances, back to back
+int rs_save_ciphertexts(void *h, const char *path, int32_t count, const int32_t *raw, const double *variances) {
+    RsKeys *keys = static_cast<RsKeys *>(h);
+    const int32_t n = io_params(keys)->n;
+    FILE *F = std::fopen(path, "wb");
+    if (!F) return -1;
+    LweSample *s = new_gate_bootstrapping_ciphertext(keys->params);
+    for (int32_t g = 0; g < count; g++) {
+        load_lwe(s, raw + (size_t)g * (n + 1), n);
+        s->current_variance = variances[g];
+        export_gate_bootstrapping_ciphertext_toFile(F, s, keys->params);
+    }
+    delete_gate_bootstrapping_ciphertext(s);
+    return std::fclose(F);
+}
+
+int rs_load_ciphertexts(void *h, const char *path, int32_t count, int32_t *raw, double *variances) {
+    RsKeys *keys = static_cast<RsKeys *>(h);
+    const int32_t n = io_params(keys)->n;
+    FILE *F = std::fopen(path, "rb");
+    if (!F) return -1;
+    LweSample *s = new_gate_bootstrapping_ciphertext(keys->params);
+    for (int32_t g = 0; g < count; g++) {
+        import_gate_bootstrapping_ciphertext_fromFile(F, s, keys->params);
+        store_lwe(raw + (size_t)g * (n + 1), s, n);
+        variances[g] = s->current_variance;
+    }
+    delete_gate_bootstrapping_ciphertext(s);
+    return std::fclose(F);
+}
+
+// A key handle from a secret keyset file (parameters from the file, owned by the reference).
+void *rs_load_secret_keyset(const char *path) {
+    FILE *F = std::fopen(path, "rb");
+    if (!F) return nullptr;
+    RsKeys *keys = new RsKeys();
+    keys->sk = new_tfheGateBootstrappingSecretKeySet_fromFile(F);
+    keys->params = const_cast<TFheGateBootstrappingParameterSet *>(keys->sk->params);
+    std::fclose(F);
+    return keys;
+}
+
+}  // extern "C"

@@ -89,6 +89,27 @@ class RefKeys:
     def bench_gates(self, code, threads, per_thread, a, b, c, out):
         return self.lib.rs_bench_gates(self.h, code, threads, per_thread, _p(a), _p(b), _p(c), _p(out))
 
+    # the reference's own file format (tfhe_io.cpp FILE* functions)
+    def save_params(self, path):
+        assert self.lib.rs_save_params(self.h, path.encode()) == 0
+
+    def save_secret_keyset(self, path):
+        assert self.lib.rs_save_secret_keyset(self.h, path.encode()) == 0
+
+    def save_cloud_keyset(self, path):
+        assert self.lib.rs_save_cloud_keyset(self.h, path.encode()) == 0
+
+    def save_ciphertexts(self, path, cts, variances):
+        cts = _i32(cts)
+        v = np.ascontiguousarray(variances, dtype=np.float64)
+        assert self.lib.rs_save_ciphertexts(self.h, path.encode(), len(cts), _p(cts), _p(v)) == 0
+
+    def load_ciphertexts(self, path, count):
+        out = np.zeros((count, self.n + 1), np.int32)
+        v = np.zeros(count, np.float64)
+        assert self.lib.rs_load_ciphertexts(self.h, path.encode(), count, _p(out), _p(v)) == 0
+        return out, v
+
     def free(self):
         if self.h is not None:
             self.lib.rs_free(self.h)
@@ -105,6 +126,12 @@ class RefLib:
         L.rs_bench_gates.restype = ctypes.c_double
         L.rs_bench_gates.argtypes = [_V, ctypes.c_int, _I, _I, _V, _V, _V, _V]
         L.rs_dtot32.argtypes = [ctypes.c_double]
+        L.rs_load_secret_keyset.restype = _V
+        L.rs_load_secret_keyset.argtypes = [ctypes.c_char_p]
+        for f in ("rs_save_params", "rs_save_secret_keyset", "rs_save_cloud_keyset"):
+            getattr(L, f).argtypes = [_V, ctypes.c_char_p]
+        L.rs_save_ciphertexts.argtypes = [_V, ctypes.c_char_p, _I, _V, _V]
+        L.rs_load_ciphertexts.argtypes = [_V, ctypes.c_char_p, _I, _V, _V]
         self.L = L
 
     @classmethod
@@ -128,6 +155,12 @@ class RefLib:
             p = custom
             h = self.L.rs_keygen(1, p["n"], p["N"], p["k"], p["l"], p["Bgbit"], p["ks_t"], p["ks_basebit"],
                                  ks_stdev, bk_stdev, seed)
+        return RefKeys(self.L, h)
+
+    def load_secret_keyset(self, path):
+        """new_tfheGateBootstrappingSecretKeySet_fromFile on a file (parameters from the file)."""
+        h = self.L.rs_load_secret_keyset(os.fsencode(path))
+        assert h, f"reference could not open {path}"
         return RefKeys(self.L, h)
 
     def modswitch_from(self, phase, msize):

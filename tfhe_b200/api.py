@@ -76,6 +76,16 @@ def lib():
         L.tfheb_set_br_variant.argtypes = [_V, _I32, _I32]
         L.tfheb_autotune.argtypes = [_V, _I32, _I32, _V, _I32]
         L.tfheb_set_keyswitch_kernel.argtypes = [_V, _I32]
+        L.tfheb_cloud_key_params.argtypes = [_V, ctypes.POINTER(Params)]
+        _C = ctypes.c_char_p
+        L.tfheb_params_save.argtypes = [_C, ctypes.POINTER(Params)]
+        L.tfheb_params_load.argtypes = [_C, ctypes.POINTER(Params)]
+        L.tfheb_cloud_key_save.argtypes = [_V, _C]
+        L.tfheb_cloud_key_load.argtypes = [_C, ctypes.POINTER(_V)]
+        L.tfheb_secret_keyset_save.argtypes = [_V, _V, _C]
+        L.tfheb_secret_keyset_load.argtypes = [_C, ctypes.POINTER(_V), ctypes.POINTER(_V)]
+        L.tfheb_ciphertexts_save.argtypes = [_C, ctypes.POINTER(Params), _I32, _V, _V]
+        L.tfheb_ciphertexts_load.argtypes = [_C, ctypes.POINTER(Params), _I32, _V, _V]
         _lib = L
     return _lib
 
@@ -254,6 +264,64 @@ def keygen(params, seed=1):
     sk, ck = _V(), _V()
     _check(lib().tfheb_keygen(ctypes.byref(params), seed, ctypes.byref(sk), ctypes.byref(ck)), "tfheb_keygen")
     return SecretKey(sk.value, params), CloudKey(ck.value, params)
+
+
+# ---- files in the reference's format (tfhe_io.cpp) -------------------------------------------
+
+def _path(path):
+    return os.fsencode(path)
+
+
+def save_params(path, params):
+    _check(lib().tfheb_params_save(_path(path), ctypes.byref(params)), "tfheb_params_save")
+
+
+def load_params(path):
+    p = Params()
+    _check(lib().tfheb_params_load(_path(path), ctypes.byref(p)), "tfheb_params_load")
+    return p
+
+
+def _cloud_params(h):
+    p = Params()
+    _check(lib().tfheb_cloud_key_params(h, ctypes.byref(p)), "tfheb_cloud_key_params")
+    return p
+
+
+def save_cloud_keyset(path, ck):
+    _check(lib().tfheb_cloud_key_save(ck.h, _path(path)), "tfheb_cloud_key_save")
+
+
+def load_cloud_keyset(path):
+    h = _V()
+    _check(lib().tfheb_cloud_key_load(_path(path), ctypes.byref(h)), "tfheb_cloud_key_load")
+    return CloudKey(h.value, _cloud_params(h))
+
+
+def save_secret_keyset(path, sk, ck):
+    _check(lib().tfheb_secret_keyset_save(sk.h, ck.h, _path(path)), "tfheb_secret_keyset_save")
+
+
+def load_secret_keyset(path):
+    s, c = _V(), _V()
+    _check(lib().tfheb_secret_keyset_load(_path(path), ctypes.byref(s), ctypes.byref(c)), "tfheb_secret_keyset_load")
+    p = _cloud_params(c)
+    return SecretKey(s.value, p), CloudKey(c.value, p)
+
+
+def save_ciphertexts(path, params, cts, variances=None):
+    cts = _i32(cts).reshape(-1, params.n + 1)
+    v = None if variances is None else np.ascontiguousarray(variances, dtype=np.float64)
+    _check(lib().tfheb_ciphertexts_save(_path(path), ctypes.byref(params), len(cts), _p(cts), _p(v)),
+           "tfheb_ciphertexts_save")
+
+
+def load_ciphertexts(path, params, count):
+    out = np.zeros((count, params.n + 1), np.int32)
+    v = np.zeros(count, np.float64)
+    _check(lib().tfheb_ciphertexts_load(_path(path), ctypes.byref(params), count, _p(out), _p(v)),
+           "tfheb_ciphertexts_load")
+    return out, v
 
 
 class Netlist:

@@ -64,9 +64,10 @@ T *make(const T &v) {  // objects with const members: construct once, copy bytes
     return p;
 }
 
-TFheGateBootstrappingParameterSet *make_params(const tfheb_params &p, double max_stdev) {
-    LweParams *in = make(LweParams{p.n, p.ks_stdev, max_stdev});
-    TLweParams *acc = make(TLweParams{p.N, p.k, p.bk_stdev, max_stdev, LweParams{p.k * p.N, p.bk_stdev, max_stdev}});
+TFheGateBootstrappingParameterSet *make_params(const tfheb_params &p, double in_alpha_max, double tlwe_alpha_max) {
+    LweParams *in = make(LweParams{p.n, p.ks_stdev, in_alpha_max});
+    TLweParams *acc = make(TLweParams{p.N, p.k, p.bk_stdev, tlwe_alpha_max,
+                                      LweParams{p.k * p.N, p.bk_stdev, tlwe_alpha_max}});
     Torus32 *h = static_cast<Torus32 *>(std::malloc(sizeof(Torus32) * p.l));
     uint32_t sum = 0;
     for (int i = 0; i < p.l; i++) {
@@ -77,6 +78,21 @@ TFheGateBootstrappingParameterSet *make_params(const tfheb_params &p, double max
     TGswParams *gp = make(TGswParams{p.l, p.Bgbit, Bg, Bg / 2, (uint32_t)(Bg - 1), acc, (p.k + 1) * p.l, h,
                                      sum * (uint32_t)(Bg / 2)});
     return make(TFheGateBootstrappingParameterSet{p.ks_t, p.ks_basebit, in, gp});
+}
+
+// The drop-in objects around an engine key pair (the keysets own sk and ck).
+TFheGateBootstrappingCloudKeySet assemble_cloud(const TFheGateBootstrappingParameterSet *params, tfheb_cloud_key *ck) {
+    const tfheb_params p = to_params(params);
+    return TFheGateBootstrappingCloudKeySet{params, new LweBootstrappingKey{ck},
+                                            new LweBootstrappingKeyFFT{ck, p.n, p.k * p.N, 0}};
+}
+TFheGateBootstrappingSecretKeySet *assemble_secret_keyset(const TFheGateBootstrappingParameterSet *params,
+                                                          tfheb_secret_key *sk, tfheb_cloud_key *ck) {
+    const int32_t n = params->in_out_params->n;
+    int32_t *key = static_cast<int32_t *>(std::malloc(sizeof(int32_t) * n));
+    tfheb_secret_key_export(sk, key, nullptr);
+    LweKey *lk = make(LweKey{params->in_out_params, key});
+    return make(TFheGateBootstrappingSecretKeySet{params, lk, new TGswKey{sk}, assemble_cloud(params, ck)});
 }
 
 LweBootstrappingKeyFFT *ready(const TFheGateBootstrappingCloudKeySet *bk) {
@@ -136,7 +152,7 @@ TFheGateBootstrappingParameterSet *new_default_gate_bootstrapping_parameters(int
     tfheb_params p;
     if (tfheb_default_params(minimum_lambda, &p) != TFHEB_OK)
         die("the requested security parameter must be in (0, 128]");
-    return make_params(p, 0.012467);
+    return make_params(p, 0.012467, 0.012467);
 }
 
 void delete_gate_bootstrapping_parameters(TFheGateBootstrappingParameterSet *params) {
@@ -154,13 +170,7 @@ TFheGateBootstrappingSecretKeySet *new_random_gate_bootstrapping_secret_keyset(
     tfheb_secret_key *sk = nullptr;
     tfheb_cloud_key *ck = nullptr;
     if (tfheb_keygen(&p, next_seed(), &sk, &ck) != TFHEB_OK) die("key generation");
-    int32_t *key = static_cast<int32_t *>(std::malloc(sizeof(int32_t) * p.n));
-    tfheb_secret_key_export(sk, key, nullptr);
-    LweKey *lk = make(LweKey{params->in_out_params, key});
-    TGswKey *gk = new TGswKey{sk};
-    LweBootstrappingKey *b = new LweBootstrappingKey{ck};
-    LweBootstrappingKeyFFT *f = new LweBootstrappingKeyFFT{ck, p.n, p.k * p.N, 0};
-    return make(TFheGateBootstrappingSecretKeySet{params, lk, gk, TFheGateBootstrappingCloudKeySet{params, b, f}});
+    return assemble_secret_keyset(params, sk, ck);
 }
 
 void delete_gate_bootstrapping_cloud_keyset(TFheGateBootstrappingCloudKeySet *keyset) {
@@ -342,6 +352,118 @@ void tfhe_bootstrap_FFT(LweSample *result, const LweBootstrappingKeyFFT *bk, Tor
 
 void tfhe_bootstrap_woKS_FFT(LweSample *result, const LweBootstrappingKeyFFT *bk, Torus32 mu, const LweSample *x) {
     bootstrap_one(result, bk, mu, x, false);
+}
+
+}  // extern "C"
+
+// ================================================================================================
+// files in the reference's format (tfhe_io.cpp:90-136, 1010-1220)
+// ================================================================================================
+
+namespace {
+
+// Parameter sets read together with a key set belong to the library, as the reference registers
+// them with its garbage collector (tfhe_io.cpp:1103-1110, 1157-1164); they are freed at exit.
+struct OwnedParams {
+    std::mutex mu;
+    std::vector<TFheGateBootstrappingParameterSet *> sets;
+    ~OwnedParams() {
+        for (auto *p : sets) delete_gate_bootstrapping_parameters(p);
+    }
+} g_owned_params;
+
+tfheb::ParamMeta meta_of(const TFheGateBootstrappingParameterSet *ps) {
+    return {ps->in_out_params->alpha_max, ps->tgsw_params->tlwe_params->alpha_max};
+}
+
+TFheGateBootstrappingParameterSet *read_params_or_die(FILE *F, tfheb::ParamMeta &m) {
+    tfheb_params p{};
+    if (!F || !tfheb::io::read_params(F, p, m)) die("reading a gate-bootstrapping parameter set");
+    return make_params(p, m.in_alpha_max, m.tlwe_alpha_max);
+}
+
+const TFheGateBootstrappingParameterSet *read_owned_params(FILE *F, tfheb::ParamMeta &m) {
+    TFheGateBootstrappingParameterSet *ps = read_params_or_die(F, m);
+    std::lock_guard<std::mutex> lock(g_owned_params.mu);
+    g_owned_params.sets.push_back(ps);
+    return ps;
+}
+
+tfheb_cloud_key *read_cloud_or_die(FILE *F, const TFheGateBootstrappingParameterSet *ps, const tfheb::ParamMeta &m) {
+    auto *c = new tfheb_cloud_key();
+    c->ck.meta = m;
+    tfheb_params p = to_params(ps);
+    if (!tfheb::io::read_cloud_content(F, p, c->ck)) die("reading a bootstrapping key");
+    return c;
+}
+
+void write_params_or_die(FILE *F, const TFheGateBootstrappingParameterSet *ps) {
+    if (!F || !tfheb::io::write_params(F, to_params(ps), meta_of(ps))) die("writing a parameter set");
+}
+
+void write_cloud_or_die(FILE *F, const TFheGateBootstrappingCloudKeySet *ks) {
+    if (!ks->bkFFT || !ks->bkFFT->ck) die("cloud keyset has no key");
+    if (!tfheb::io::write_cloud_content(F, ks->bkFFT->ck->ck)) die("writing a bootstrapping key");
+}
+
+}  // namespace
+
+extern "C" {
+
+void export_lweSample_toFile(FILE *F, const LweSample *sample, const LweParams *params) {
+    if (!F || !tfheb::io::write_lwe_sample(F, params->n, sample->a, sample->b, sample->current_variance))
+        die("writing a LWE sample");
+}
+
+void import_lweSample_fromFile(FILE *F, LweSample *sample, const LweParams *params) {
+    if (!F || !tfheb::io::read_lwe_sample(F, params->n, sample->a, &sample->b, &sample->current_variance))
+        die("reading a LWE sample");
+}
+
+void export_gate_bootstrapping_ciphertext_toFile(FILE *F, const LweSample *sample,
+                                                 const TFheGateBootstrappingParameterSet *params) {
+    export_lweSample_toFile(F, sample, params->in_out_params);
+}
+
+void import_gate_bootstrapping_ciphertext_fromFile(FILE *F, LweSample *sample,
+                                                   const TFheGateBootstrappingParameterSet *params) {
+    import_lweSample_fromFile(F, sample, params->in_out_params);
+}
+
+void export_tfheGateBootstrappingParameterSet_toFile(FILE *F, const TFheGateBootstrappingParameterSet *params) {
+    write_params_or_die(F, params);
+}
+
+TFheGateBootstrappingParameterSet *new_tfheGateBootstrappingParameterSet_fromFile(FILE *F) {
+    tfheb::ParamMeta m;
+    return read_params_or_die(F, m);
+}
+
+void export_tfheGateBootstrappingCloudKeySet_toFile(FILE *F, const TFheGateBootstrappingCloudKeySet *keyset) {
+    write_params_or_die(F, keyset->params);
+    write_cloud_or_die(F, keyset);
+}
+
+TFheGateBootstrappingCloudKeySet *new_tfheGateBootstrappingCloudKeySet_fromFile(FILE *F) {
+    tfheb::ParamMeta m;
+    const TFheGateBootstrappingParameterSet *ps = read_owned_params(F, m);
+    return make(assemble_cloud(ps, read_cloud_or_die(F, ps, m)));
+}
+
+void export_tfheGateBootstrappingSecretKeySet_toFile(FILE *F, const TFheGateBootstrappingSecretKeySet *keyset) {
+    write_params_or_die(F, keyset->params);
+    write_cloud_or_die(F, &keyset->cloud);
+    if (!keyset->tgsw_key || !tfheb::io::write_secret_content(F, keyset->tgsw_key->sk->sk))
+        die("writing the secret keys");
+}
+
+TFheGateBootstrappingSecretKeySet *new_tfheGateBootstrappingSecretKeySet_fromFile(FILE *F) {
+    tfheb::ParamMeta m;
+    const TFheGateBootstrappingParameterSet *ps = read_owned_params(F, m);
+    tfheb_cloud_key *ck = read_cloud_or_die(F, ps, m);
+    auto *sk = new tfheb_secret_key();
+    if (!tfheb::io::read_secret_content(F, ck->ck.p, sk->sk)) die("reading the secret keys");
+    return assemble_secret_keyset(ps, sk, ck);
 }
 
 }  // extern "C"

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <cstdio>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -49,8 +50,17 @@ struct DeviceKsk {
     int tile_slots = 0;        // resident CTAs of the tiled kernel on the device
 };
 
+// What a reference parameter file carries beyond tfheb_params: the LWE and TLWE alpha_max
+// (0.012467 in the reference's default sets, tfhe_gate_bootstrapping.cpp:26-75).
+struct ParamMeta {
+    double in_alpha_max = 0.012467;
+    double tlwe_alpha_max = 0.012467;
+};
+
 struct CloudKey {
     tfheb_params p{};
+    ParamMeta meta;
+    double ks_var = -1, bk_var = -1;  // stored key variances of a loaded file (< 0: stdev^2 on save)
     std::vector<int32_t> bsk_coef;  // [n][kpl][k+1][N] coefficient domain (host)
     std::vector<int32_t> ksk;       // [kN][t][base][n+1] (host)
     // device state
@@ -141,6 +151,18 @@ tfheb_status prepare_device(CloudKey &ck, int precision);
 void gate_form(int gate, int32_t *cst, int32_t *sa, int32_t *sb);
 int bara_stride_for(const tfheb_params &p);
 extern std::atomic<int64_t> g_kernel_launches;
+
+// ---- reference file format (io.cu) ----------------------------------------------------------
+namespace io {
+bool write_params(FILE *f, const tfheb_params &p, const ParamMeta &m);
+bool read_params(FILE *f, tfheb_params &p, ParamMeta &m);
+bool write_cloud_content(FILE *f, const CloudKey &ck);
+bool read_cloud_content(FILE *f, tfheb_params &p, CloudKey &ck);
+bool write_secret_content(FILE *f, const SecretKey &sk);
+bool read_secret_content(FILE *f, const tfheb_params &p, SecretKey &sk);
+bool write_lwe_sample(FILE *f, int32_t n, const int32_t *a, int32_t b, double variance);
+bool read_lwe_sample(FILE *f, int32_t n, int32_t *a, int32_t *b, double *variance);
+}  // namespace io
 
 // ---- errors ---------------------------------------------------------------------------------
 void set_error(const std::string &msg);
