@@ -202,9 +202,10 @@ tfheb_status tfheb_br_variants(int32_t N, int32_t precision, int32_t *teams_per_
 tfheb_status tfheb_set_br_variant(tfheb_cloud_key *ck, int32_t precision, int32_t variant);
 tfheb_status tfheb_autotune(tfheb_cloud_key *ck, int32_t precision, int32_t boots, double *ms, int32_t cap);
 
-/* Keyswitch kernel of a key: 0 = default (tiled when the parameter set has a tiled instantiation,
- * ks_t = 8 and basebit = 2), 1 = one CTA per sample, 2 = tiled (TFHEB_ERR_UNSUPPORTED without a
- * tiled instantiation).  Both give the reference's lweKeySwitch result bit for bit; the choice is a
+/* Keyswitch kernel of a key: 0 = default, 1 = one CTA per sample, 2 = tiled (key rows shared
+ * through shared memory), 3 = register-key (key rows held in registers across samples); 2 and 3
+ * need ks_t = 8 and basebit = 2 (TFHEB_ERR_UNSUPPORTED otherwise), which the default also uses
+ * when it can.  Both give the reference's lweKeySwitch result bit for bit; the choice is a
  * performance knob.  No reference counterpart. */
 tfheb_status tfheb_set_keyswitch_kernel(tfheb_cloud_key *ck, int32_t which);
 

@@ -97,14 +97,16 @@ def _keyswitch_with(ck, p, x, which, fill):
 # batch sizes: 1 and 63 split the coefficient range over CTAs (atomic combination), 64/65/300 give
 # full and ragged 64-sample tiles, 2100 more tiles than one wave of CTAs
 @pytest.mark.parametrize("count", [1, 63, 64, 65, 300, 2100])
-def test_keyswitch_tiled_equals_per_sample_kernel(oracle, default_keys, count):
+def test_keyswitch_kernels_agree_bit_for_bit(oracle, default_keys, count):
     p, sk, ck, bsk, ksk = default_keys
     rng = np.random.default_rng(100 + count)
     x = rng.integers(-2**31, 2**31, (count, p.k * p.N + 1), dtype=np.int64).astype(np.int32)
     x[0] = -1
     per_sample = _keyswitch_with(ck, p, x, 1, 0)
     tiled = _keyswitch_with(ck, p, x, 2, -7)  # garbage in the output rows must not leak through
+    regkey = _keyswitch_with(ck, p, x, 3, 13)
     assert (tiled == per_sample).all()
+    assert (regkey == per_sample).all()
     pick = sorted({0, count - 1, count // 2})
     assert (tiled[pick] == oracle.keyswitch(pdict(p), ksk, x[pick])).all()
 
@@ -115,6 +117,7 @@ def test_keyswitch_tiled_large_params_bit_exact(oracle, large_keys):
     x = rng.integers(-2**31, 2**31, (130, p.k * p.N + 1), dtype=np.int64).astype(np.int32)
     tiled = _keyswitch_with(ck, p, x, 2, 5)
     assert (tiled == _keyswitch_with(ck, p, x, 1, 0)).all()
+    assert (tiled == _keyswitch_with(ck, p, x, 3, -3)).all()
     assert (tiled[[0, 129]] == oracle.keyswitch(pdict(p), ksk, x[[0, 129]])).all()
 
 

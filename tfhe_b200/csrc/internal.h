@@ -48,6 +48,10 @@ struct DeviceKsk {
     int tile_cw = 0;           // output columns per warp of the tiled kernel (0: tiled kernel unavailable)
     int tile_slices = 0;       // column slices of 4 * tile_cw columns covering n+1
     int tile_slots = 0;        // resident CTAs of the tiled kernel on the device
+    int32_t *rk = nullptr;     // register-key kernel: [slice][kN][t][base-1][32*rk_c]
+    int rk_c = 0;              // output columns per lane of the register-key kernel (0: unavailable)
+    int rk_slices = 0;         // column blocks of 32 * rk_c columns covering n+1
+    int rk_slots = 0;          // resident CTAs of the register-key kernel on the device
 };
 
 // What a reference parameter file carries beyond tfheb_params: the LWE and TLWE alpha_max
@@ -67,7 +71,7 @@ struct CloudKey {
     int device = -1;
     DeviceBsk dbsk[2];              // [TFHEB_FP64], [TFHEB_SPLIT_FP32]
     DeviceKsk dksk;
-    int ks_kernel = 0;              // 0 = choose by batch size, 1 = per-gate, 2 = tiled
+    int ks_kernel = 0;              // 0 = default, 1 = per-sample, 2 = tiled, 3 = register-key
     cudaStream_t stream = nullptr;
     // scratch (grown on demand)
     int32_t *d_bara = nullptr;

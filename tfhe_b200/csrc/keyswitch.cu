@@ -243,6 +243,165 @@ __global__ void __launch_bounds__(kKsThreads, 2)
 }
 
 // ============================================================================================
+// register-key kernel
+// ============================================================================================
+//
+// One CTA of 8 warps per (8*G samples, block of 32*C output columns, range of input coefficients).
+// Lane = column pair: lane l owns columns 64*p + 2*l + {0, 1}, p < C/2, so every shared load and
+// global store of a warp touches consecutive words.  Per input coefficient i the block's key rows
+// (t x 3 non-zero digits x 32*C columns) arrive in one bulk copy; per digit position j each lane
+// loads its 3*C key words into registers once and applies them to the G samples of its warp.  A
+// sample's digit is the same in every lane, so selecting the row is a warp-uniform branch and a
+// zero digit costs no additions.  This lifts the one-word-per-subtraction shared-memory bound of
+// the tiled kernel: each loaded word serves G samples.
+
+template <int C, int G>
+struct KsRegKey {
+    static_assert(C % 2 == 0, "columns per lane come in pairs");
+    static constexpr int block = 32 * C;                       // output columns per CTA
+    static constexpr int rows = kKsT * (kKsBase - 1);          // non-zero digit rows per coefficient
+    static constexpr int stage_words = rows * block;           // [j][digit 1..3][block]
+    static constexpr int stage_bytes = 4 * stage_words;
+    static constexpr int stages = stage_bytes <= 32768 ? 3 : 2;
+    static constexpr int warps = 8;
+    static constexpr int tile = warps * G;                     // samples per CTA
+    static constexpr int sa_ld = tile + 1;
+    static constexpr int ring_off = 128;                       // [0, 24): full barriers, [64]: abort flag
+    static constexpr int sa_off = ring_off + stages * stage_bytes;
+    static constexpr int smem_bytes = sa_off + 4 * kKsChunk * sa_ld;
+    static_assert(stage_bytes % 16 == 0, "bulk copies need 16-byte sizes");
+};
+
+template <int C, int G>
+__global__ void __launch_bounds__(256, 1)
+    keyswitch_regkey_kernel(const int32_t *__restrict__ rows, const uint32_t *__restrict__ in, int in_stride,
+                            uint32_t *__restrict__ out, int count, int n, int kN, int slices, int ksplit,
+                            int chunk_len, uint64_t timeout_ns, int32_t *err) {
+    using L = KsRegKey<C, G>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int kchunk = blockIdx.x % ksplit;
+    const int unit = blockIdx.x / ksplit;
+    const int slice = unit % slices, tile = unit / slices;
+    const int i_begin = kchunk * chunk_len;
+    const int i_count = min(kN, i_begin + chunk_len) - i_begin;
+
+    const uint32_t bars = smem_addr(smem);
+    volatile int32_t *abort_flag = reinterpret_cast<volatile int32_t *>(smem + 64);
+    const uint32_t *ring = reinterpret_cast<const uint32_t *>(smem + L::ring_off);
+    uint32_t *s_a = reinterpret_cast<uint32_t *>(smem + L::sa_off);
+    if (tid == 0) {
+        for (int s = 0; s < L::stages; s++) mbar_init(bars + 8 * s, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const int32_t *src = rows + ((size_t)slice * kN + i_begin) * L::stage_words;
+    auto issue = [&](int q, int s) {
+        const uint32_t bar = bars + 8 * s;
+        mbar_arrive_expect_tx(bar, L::stage_bytes);
+        bulk_copy_g2s(smem_addr(ring + s * L::stage_words), src + (size_t)q * L::stage_words, L::stage_bytes, bar);
+    };
+    int issued = 0;  // meaningful in thread 0 only
+    if (tid == 0)
+        for (; issued < L::stages && issued < i_count; issued++) issue(issued, issued);
+
+    uint32_t acc[G][C];
+#pragma unroll
+    for (int s = 0; s < G; s++)
+#pragma unroll
+        for (int c = 0; c < C; c++) acc[s][c] = 0;
+    const uint32_t prec_offset = 1u << (32 - (1 + 2 * kKsT));  // lwe-keyswitch-functions.cpp:119
+    int q = 0;
+    bool failed = false;
+    for (; q < i_count; q++) {
+        if ((q & (kKsChunk - 1)) == 0) {
+            // stage the next kKsChunk mask coefficients of the tile's samples, [coef][sample]
+            __syncthreads();
+            for (int e = tid; e < L::tile * kKsChunk; e += 256) {
+                const int g = e / kKsChunk, ii = e - g * kKsChunk;
+                const int gg = tile * L::tile + g;
+                uint32_t v = 0;
+                if (gg < count && q + ii < i_count) v = in[(size_t)gg * in_stride + i_begin + q + ii] + prec_offset;
+                s_a[ii * L::sa_ld + g] = v;
+            }
+            __syncthreads();
+        }
+        const int st_i = q % L::stages;
+        const bool ok = wait_bounded(bars + 8 * st_i, (q / L::stages) & 1, abort_flag, timeout_ns, err);
+        uint32_t abar[G];
+#pragma unroll
+        for (int s = 0; s < G; s++) abar[s] = s_a[(q & (kKsChunk - 1)) * L::sa_ld + warp * G + s];
+        const uint32_t *stage = ring + st_i * L::stage_words + 2 * lane;
+#pragma unroll 1
+        for (int j = 0; j < kKsT; j++) {
+            uint32_t k1[C], k2[C], k3[C];
+            const uint32_t *rj = stage + j * (kKsBase - 1) * L::block;
+#pragma unroll
+            for (int p = 0; p < C / 2; p++) {
+                const uint2 v1 = *reinterpret_cast<const uint2 *>(rj + 64 * p);
+                const uint2 v2 = *reinterpret_cast<const uint2 *>(rj + L::block + 64 * p);
+                const uint2 v3 = *reinterpret_cast<const uint2 *>(rj + 2 * L::block + 64 * p);
+                k1[2 * p] = v1.x, k1[2 * p + 1] = v1.y;
+                k2[2 * p] = v2.x, k2[2 * p + 1] = v2.y;
+                k3[2 * p] = v3.x, k3[2 * p + 1] = v3.y;
+            }
+            const int sh = 30 - 2 * j;  // digit j from the top (lwe-keyswitch-functions.cpp:128-131)
+#pragma unroll
+            for (int s = 0; s < G; s++) {
+                const uint32_t d = (abar[s] >> sh) & 3u;  // the same in every lane of the warp
+                if (d == 1) {
+#pragma unroll
+                    for (int c = 0; c < C; c++) acc[s][c] -= k1[c];
+                } else if (d == 2) {
+#pragma unroll
+                    for (int c = 0; c < C; c++) acc[s][c] -= k2[c];
+                } else if (d == 3) {
+#pragma unroll
+                    for (int c = 0; c < C; c++) acc[s][c] -= k3[c];
+                }
+            }
+        }
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        if (tid == 0 && issued < i_count) {
+            issue(issued, st_i);
+            issued++;
+        }
+    }
+    if (failed) {
+        // drain the copies still in flight before the CTA exits (each wait bounded)
+        if (tid == 0) {
+            volatile int32_t no_abort = 0;
+            for (int r = q; r < issued; r++)
+                wait_bounded(bars + 8 * (r % L::stages), (r / L::stages) & 1, &no_abort, timeout_ns, err);
+        }
+        return;
+    }
+
+    const int ncols = n + 1;
+#pragma unroll
+    for (int s = 0; s < G; s++) {
+        const int g = tile * L::tile + warp * G + s;
+        if (g >= count) break;
+        uint32_t *o = out + (size_t)g * ncols;
+        const uint32_t b = kchunk == 0 ? in[(size_t)g * in_stride + kN] : 0u;
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const int col = slice * L::block + 64 * (c >> 1) + 2 * lane + (c & 1);
+            if (col >= ncols) continue;
+            // result = (0, b) - sum  (lwe-keyswitch-functions.cpp:233-237)
+            const uint32_t v = acc[s][c] + (col == n ? b : 0u);
+            if (ksplit == 1) o[col] = v;
+            else atomicAdd(o + col, v);
+        }
+    }
+}
+
+// ============================================================================================
 // host side
 // ============================================================================================
 
@@ -303,6 +462,61 @@ cudaError_t tiled_slots(int device, int *slots) {
     return cudaSuccess;
 }
 
+// register-key instantiations: columns per lane C and samples per warp G
+constexpr int kRkC[] = {10, 14};
+int rk_samples_per_warp(int c) { return c == 10 ? 7 : 5; }
+
+int choose_rk_c(int n) {
+    int best = 0, best_cols = 0;
+    for (int c : kRkC) {
+        const int block = 32 * c;
+        const int cols = (n + 1 + block - 1) / block * block;
+        if (!best || cols < best_cols) best = c, best_cols = cols;
+    }
+    return best;
+}
+
+template <int C, int G>
+cudaError_t regkey_slots(int device, int *slots) {
+    using L = KsRegKey<C, G>;
+    cudaError_t e = cudaFuncSetAttribute(keyswitch_regkey_kernel<C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         L::smem_bytes);
+    if (e != cudaSuccess) return e;
+    int occ = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, keyswitch_regkey_kernel<C, G>, 256, L::smem_bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    *slots = std::max(occ, 1) * sms;
+    return cudaSuccess;
+}
+
+template <int C, int G>
+cudaError_t launch_regkey(const CloudKey &ck, int count, const int32_t *in, int in_stride, int32_t *out,
+                          cudaStream_t s) {
+    using L = KsRegKey<C, G>;
+    const tfheb_params &p = ck.p;
+    const int kN = p.k * p.N;
+    cudaError_t e = cudaFuncSetAttribute(keyswitch_regkey_kernel<C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         L::smem_bytes);
+    if (e != cudaSuccess) return e;
+    const int tiles = (count + L::tile - 1) / L::tile;
+    const int units = tiles * ck.dksk.rk_slices;
+    // split the coefficient range only when the units alone leave resident slots idle
+    int ksplit = std::max(1, std::min(ck.dksk.rk_slots / units, kN / kKsChunk));
+    int chunk_len = (kN + ksplit - 1) / ksplit;
+    chunk_len = (chunk_len + kKsChunk - 1) / kKsChunk * kKsChunk;
+    ksplit = (kN + chunk_len - 1) / chunk_len;
+    if (ksplit > 1) {
+        e = cudaMemsetAsync(out, 0, (size_t)count * (p.n + 1) * sizeof(int32_t), s);
+        if (e != cudaSuccess) return e;
+    }
+    keyswitch_regkey_kernel<C, G><<<units * ksplit, 256, L::smem_bytes, s>>>(
+        ck.dksk.rk, reinterpret_cast<const uint32_t *>(in), in_stride, reinterpret_cast<uint32_t *>(out), count,
+        p.n, kN, ck.dksk.rk_slices, ksplit, chunk_len, ck.wait_timeout_ns, ck.d_err);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t upload_keyswitch_key(CloudKey &ck) {
@@ -341,12 +555,35 @@ cudaError_t upload_keyswitch_key(CloudKey &ck) {
         d.tile_cw = cw;
         d.tile_slices = slices;
     }
+    if (!d.rk && tiled_params(p)) {
+        const int c = choose_rk_c(p.n);
+        const int block = 32 * c;
+        const int slices = (ncols + block - 1) / block;
+        // [slice][i][j][digit 1..3][block]; columns past n are zero
+        std::vector<int32_t> rk((size_t)slices * kN * t * (base - 1) * block, 0);
+        for (int sl = 0; sl < slices; sl++)
+            for (int i = 0; i < kN; i++)
+                for (int j = 0; j < t; j++)
+                    for (int h = 1; h < base; h++) {
+                        const int32_t *srow = &ck.ksk[(((size_t)i * t + j) * base + h) * ncols];
+                        int32_t *drow = &rk[((((size_t)sl * kN + i) * t + j) * (base - 1) + (h - 1)) * block];
+                        for (int col = 0; col < block && sl * block + col < ncols; col++)
+                            drow[col] = srow[sl * block + col];
+                    }
+        if ((e = cudaMalloc((void **)&d.rk, rk.size() * 4)) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(d.rk, rk.data(), rk.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+        e = c == 10 ? regkey_slots<10, 7>(ck.device, &d.rk_slots) : regkey_slots<14, 5>(ck.device, &d.rk_slots);
+        if (e != cudaSuccess) return e;
+        d.rk_c = c;
+        d.rk_slices = slices;
+    }
     return cudaSuccess;
 }
 
 void free_keyswitch_key(DeviceKsk &d) {
     if (d.rows) cudaFree(d.rows);
     if (d.tiles) cudaFree(d.tiles);
+    if (d.rk) cudaFree(d.rk);
     d = DeviceKsk{};
 }
 
@@ -354,6 +591,13 @@ cudaError_t launch_keyswitch(const CloudKey &ck, int count, const int32_t *in, i
                              cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
     const tfheb_params &p = ck.p;
+    if (ck.ks_kernel == 3 && ck.dksk.rk_c != 0) {
+        switch (ck.dksk.rk_c) {
+            case 10: return launch_regkey<10, 7>(ck, count, in, in_stride, out, s);
+            case 14: return launch_regkey<14, 5>(ck, count, in, in_stride, out, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     const bool tiled = ck.dksk.tile_cw != 0 && ck.ks_kernel != 1;
     if (tiled) {
         switch (ck.dksk.tile_cw) {
