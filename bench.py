@@ -43,10 +43,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["nand", "netlist", "mux2048", "errors"], default="nand",
+    ap.add_argument("--workload", choices=["nand", "netlist", "mux2048", "errors", "keyswitch"], default="nand",
                     help="nand: the headline line (4096 NAND batches); the others print their own line: "
                          "netlist = seeded 200-level random circuit through a CUDA graph, mux2048 = 1024 MUX "
-                         "at N=2048, errors = decryption-error count over 10^6 split-FP32 NAND gates")
+                         "at N=2048, errors = decryption-error count over 10^6 split-FP32 NAND gates, "
+                         "keyswitch = the three keyswitch kernels on --batch extracted samples")
     ap.add_argument("--gates", type=int, default=1_000_000, help="gate count of --workload errors")
     return ap.parse_args()
 
@@ -156,6 +157,37 @@ def run_extra_workload(args):
             batch += 1
         out.update({"form": "split-FP32", "gates": done, "decryption_errors": errors, "batches": batch,
                     "wall_s": time.perf_counter() - t0})
+    elif args.workload == "keyswitch":
+        # default parameters, --batch random extracted samples (dimension kN + 1); each kernel runs
+        # --warmup untimed then --steps timed calls on this stream; outputs must agree bit for bit
+        p = tb.default_params()
+        sk, ck = tb.keygen(p, seed=3)
+        ck.to_device(0, precisions=(tb.FP64,))
+        B = args.batch
+        rng = np.random.default_rng(B)
+        x = torch.from_numpy(rng.integers(-2**31, 2**31, (B, p.k * p.N + 1), dtype=np.int64).astype(np.int32)).cuda()
+        ref_out, times = None, {}
+        for which, name in ((1, "per_sample"), (2, "tiled"), (3, "regkey")):
+            ck.set_keyswitch_kernel(which)
+            dout = torch.zeros((B, p.n + 1), dtype=torch.int32, device="cuda")
+            for _ in range(args.warmup):
+                ck.keyswitch_device(x, dout, B, stream=sptr)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(args.steps):
+                ck.keyswitch_device(x, dout, B, stream=sptr)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times[name] = e0.elapsed_time(e1) / args.steps
+            got = dout.cpu().numpy()
+            if ref_out is None:
+                ref_out = got
+            elif not (got == ref_out).all():
+                raise RuntimeError(f"keyswitch kernel {name} disagrees with the per-sample kernel")
+        ck.set_keyswitch_kernel(0)
+        out.update({"samples": B, "ms_per_call": times, "bit_identical": True,
+                    "params": "n=630,N=1024,k=1,ks_t=8,ks_basebit=2"})
     print(json.dumps(out), flush=True)
 
 

@@ -137,6 +137,17 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *ck, int32_t device, int3
 tfheb_status tfheb_gate_batch(tfheb_cloud_key *ck, int32_t gate, int32_t precision, int32_t count,
                               const int32_t *a, const int32_t *b, const int32_t *c, int32_t *out);
 
+/* The same batch sharded across several keys, each moved to its own GPU with
+ * tfheb_cloud_key_to_device (keys with the same key material; the same device twice is allowed).
+ * Shard k is rows [count*k/nkeys, count*(k+1)/nkeys), evaluated with tfheb_gate_batch on key k in
+ * its own host thread; the output is bit-identical to one tfheb_gate_batch call.  Replica
+ * sharding only: gates of a batch are independent, so there is no exchange between GPUs.
+ * No reference counterpart (the reference evaluates gates on one CPU thread per call).  On error
+ * the message names the failing shard. */
+tfheb_status tfheb_gate_batch_multi(tfheb_cloud_key *const *cks, int32_t nkeys, int32_t gate, int32_t precision,
+                                    int32_t count, const int32_t *a, const int32_t *b, const int32_t *c,
+                                    int32_t *out);
+
 /* Same on device buffers, enqueued on `stream` (a cudaStream_t, NULL = the key's stream). */
 tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *ck, int32_t gate, int32_t precision, int32_t count,
                                      const int32_t *d_a, const int32_t *d_b, const int32_t *d_c, int32_t *d_out,

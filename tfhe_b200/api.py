@@ -77,6 +77,7 @@ def lib():
         L.tfheb_autotune.argtypes = [_V, _I32, _I32, _V, _I32]
         L.tfheb_set_keyswitch_kernel.argtypes = [_V, _I32]
         L.tfheb_cloud_key_params.argtypes = [_V, ctypes.POINTER(Params)]
+        L.tfheb_gate_batch_multi.argtypes = [_V, _I32, _I32, _I32, _I32, _V, _V, _V, _V]
         _C = ctypes.c_char_p
         L.tfheb_params_save.argtypes = [_C, ctypes.POINTER(Params)]
         L.tfheb_params_load.argtypes = [_C, ctypes.POINTER(Params)]
@@ -264,6 +265,18 @@ def keygen(params, seed=1):
     sk, ck = _V(), _V()
     _check(lib().tfheb_keygen(ctypes.byref(params), seed, ctypes.byref(sk), ctypes.byref(ck)), "tfheb_keygen")
     return SecretKey(sk.value, params), CloudKey(ck.value, params)
+
+
+def gate_batch_multi(cks, gate, a, b=None, c=None, precision=FP64):
+    """One batch of gates sharded across cloud keys on several GPUs (tfheb_gate_batch_multi)."""
+    a = _i32(a)
+    b = None if b is None else _i32(b)
+    c = None if c is None else _i32(c)
+    out = np.zeros_like(a)
+    arr = (_V * len(cks))(*[k.h for k in cks])
+    _check(lib().tfheb_gate_batch_multi(ctypes.cast(arr, _V), len(cks), gate, precision, len(a), _p(a), _p(b),
+                                        _p(c), _p(out)), "tfheb_gate_batch_multi")
+    return out
 
 
 # ---- files in the reference's format (tfhe_io.cpp) -------------------------------------------

@@ -6,7 +6,7 @@
 // with digit_j the j-th basebit-bit digit from the top.  All arithmetic is mod 2^32, so any order of
 // the additions gives the reference's result bit for bit.
 //
-// Two kernels:
+// Three kernels:
 //   keyswitch_gate_kernel   one CTA per sample, each thread 4 output columns; the selected key rows are
 //                           gathered from L2 per sample (15.5 MB of rows per sample at n = 630).  Used
 //                           for parameter sets without a tiled instantiation, or on request.
@@ -17,7 +17,10 @@
 //                           at most 4 distinct rows (digit 0 reads a zero row) and every 16-byte load
 //                           is a broadcast.  L2->SM key traffic drops from 15.5 MB per sample to 15.5 MB
 //                           per 64 samples.  Small batches split the i range over CTAs and combine the
-//                           partial sums with atomic adds (mod 2^32, exact).
+//                           partial sums with atomic adds (mod 2^32, exact).  Default below 256 samples.
+//   keyswitch_regkey_kernel lane = column pair, key rows of one (i, j) held in registers and applied to
+//                           7 samples per warp through a warp-uniform digit branch; each loaded key
+//                           word serves 7 subtractions.  Default from 256 samples.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -462,6 +465,8 @@ cudaError_t tiled_slots(int device, int *slots) {
     return cudaSuccess;
 }
 
+constexpr int kRegKeyMinCount = 256;  // default kernel switch-over (samples per call)
+
 // register-key instantiations: columns per lane C and samples per warp G
 constexpr int kRkC[] = {10, 14};
 int rk_samples_per_warp(int c) { return c == 10 ? 7 : 5; }
@@ -591,7 +596,11 @@ cudaError_t launch_keyswitch(const CloudKey &ck, int count, const int32_t *in, i
                              cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
     const tfheb_params &p = ck.p;
-    if (ck.ks_kernel == 3 && ck.dksk.rk_c != 0) {
+    // default: the register-key kernel from kRegKeyMinCount samples (measured 2.00 vs 2.88 ms per
+    // 4096 and 0.63 vs 0.74 ms per 1036 samples against the tiled kernel), the tiled kernel below
+    // (0.047 vs 0.086 ms for one sample: more CTAs share a small batch)
+    const bool regkey = ck.ks_kernel == 3 || (ck.ks_kernel == 0 && count >= kRegKeyMinCount);
+    if (regkey && ck.dksk.rk_c != 0) {
         switch (ck.dksk.rk_c) {
             case 10: return launch_regkey<10, 7>(ck, count, in, in_stride, out, s);
             case 14: return launch_regkey<14, 5>(ck, count, in, in_stride, out, s);
