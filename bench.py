@@ -136,7 +136,7 @@ def run_extra_workload(args):
                          "errors": int((got != np.where(a == 1, b, c)).sum()), "autotune": tune}
         out.update({"params": "n=800,N=2048,k=1,l=3,Bgbit=8,ks_t=8,ks_basebit=2", "batch": B,
                     "split_shift": int(tb.api.lib().tfheb_default_split_shift(ctypes.byref(p)))})
-    else:  # errors
+    elif args.workload == "errors":
         p = tb.default_params()
         sk, ck = tb.keygen(p, seed=6)
         ck.to_device(0)

@@ -129,3 +129,14 @@ def test_dropin_header_compiles_as_c_and_cxx(tmp_path):
     inc = os.path.join(ROOT, "include")
     for compiler, flags in (("gcc", ["-std=c99"]), ("g++", ["-x", "c++"])):
         subprocess.check_call([compiler, *flags, "-I", inc, "-c", str(src), "-o", str(tmp_path / "prog.o")])
+
+
+def test_bench_script_parses_and_lists_its_workloads():
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--help"], capture_output=True, text=True,
+                         timeout=120)
+    assert res.returncode == 0, res.stderr
+    for w in ("netlist", "mux2048", "errors", "keyswitch"):
+        assert w in res.stdout
