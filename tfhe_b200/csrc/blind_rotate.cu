@@ -81,7 +81,8 @@ struct BrLayout {
     static constexpr size_t tables_bytes = ((sizeof(cplx<T>) * TW) + 15) / 16 * 16;
     static constexpr size_t teams = tables + tables_bytes;
     static constexpr size_t team_acc = 4 * (size_t)KP1 * N;
-    static constexpr size_t team_buf = ((size_t)Exch<T, M>::bytes + 15) / 16 * 16;
+    static constexpr size_t team_xbuf = ((size_t)Exch<T, M>::bytes + 15) / 16 * 16;  // one exchange buffer
+    static constexpr size_t team_buf = 2 * team_xbuf;                                // the alternating pair
     __host__ __device__ static size_t team_bytes(int nsteps) {
         return team_acc + team_buf + 16 * (((size_t)nsteps + 4 + 3) / 4);
     }
@@ -180,7 +181,7 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
 
     unsigned char *tb = smem + Lay::teams + (size_t)team * Lay::team_bytes(args.nsteps);
     uint32_t *s_acc = reinterpret_cast<uint32_t *>(tb);
-    void *buf = tb + Lay::team_acc;
+    ExchPair xp{tb + Lay::team_acc, (uint32_t)Lay::team_xbuf, 0u};
     int32_t *s_bara = reinterpret_cast<int32_t *>(tb + Lay::team_acc + Lay::team_buf);
     const cplx<T> *s_tw = s_tab;
 
@@ -256,7 +257,7 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                     const T d1 = DigitConv<T>::conv((x1[r] >> shift) & maskBg, digit_bias);
                     z[r] = cplx<T>{d0, -d1};  // a_j - i a_{j+M}; the twist is folded into the FFT
                 }
-                F::forward(z, buf, s_tw, t, bar_id);
+                F::forward(z, xp, s_tw, t, bar_id);
 
                 const int s = c % D;
                 wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns, args.err);
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
 #pragma unroll
                     for (int r = 0; r < kR; r++) z[r] = acc_hi[v][r];
                 }
-                F::inverse(z, buf, s_tw, t, bar_id);
+                F::inverse(z, xp, s_tw, t, bar_id);
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
                     const cplx<T> w = z[r];  // (c_j - i c_{j+M})
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                     z[2 * m] = {acc_l[v][m].re.x, acc_l[v][m].im.x};
                     z[2 * m + 1] = {acc_l[v][m].re.y, acc_l[v][m].im.y};
                 }
-                F::inverse(z, buf, s_tw, t, bar_id);
+                F::inverse(z, xp, s_tw, t, bar_id);
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
                     const cplx<T> w = z[r];
@@ -376,9 +377,6 @@ struct BrVariant {
 };
 static const BrVariant kBrVariants[] = {
     {1024, TFHEB_SPLIT_FP32, 7, 4, launch_g<float, 1024, true, 7, 4>},
-    {1024, TFHEB_SPLIT_FP32, 7, 6, launch_g<float, 1024, true, 7, 6>},
-    {1024, TFHEB_SPLIT_FP32, 6, 4, launch_g<float, 1024, true, 6, 4>},
-    {1024, TFHEB_SPLIT_FP32, 6, 6, launch_g<float, 1024, true, 6, 6>},
     {1024, TFHEB_SPLIT_FP32, 5, 4, launch_g<float, 1024, true, 5, 4>},
     {1024, TFHEB_SPLIT_FP32, 4, 4, launch_g<float, 1024, true, 4, 4>},
     {1024, TFHEB_FP64, 3, 4, launch_g<double, 1024, false, 3, 4>},

@@ -19,7 +19,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-
 namespace tfheb {
 
 template <typename T>
@@ -258,7 +257,21 @@ __device__ __forceinline__ void team_sync(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Team FFT: T = M/R threads, t in [0,T), registers x[R], exchange buffer buf (Exch<T, M>::bytes).
+// Two exchange buffers of a team, used alternately by consecutive exchanges (the parity runs on
+// across transforms).  Exchange k stores into buffer k % 2, whose last readers (exchange k-2) all
+// passed the barrier of exchange k-1 before this store: one barrier per exchange suffices.
+struct ExchPair {
+    unsigned char *base;
+    uint32_t stride;  // bytes of one buffer
+    uint32_t parity;  // buffer of the next exchange
+    __device__ __forceinline__ void *next() {
+        void *b = base + parity * stride;
+        parity ^= 1u;
+        return b;
+    }
+};
+
+// Team FFT: T = M/R threads, t in [0,T), registers x[R], two exchange buffers (Exch<T, M>::bytes each).
 template <typename T, int M, int R>
 struct TeamFft {
     static constexpr int NT = M / R;  // threads per team
@@ -336,44 +349,44 @@ struct TeamFft {
     }
 
     template <int S>
-    __device__ static __forceinline__ void forward_from(cplx<T> *x, void *buf, const cplx<T> *tw, int t, int bar_id) {
+    __device__ static __forceinline__ void forward_from(cplx<T> *x, ExchPair &xp, const cplx<T> *tw, int t, int bar_id) {
         constexpr int r = Stage<M, S>::r;
 #pragma unroll
         for (int c = 0; c < R / r; c++) dft<T, false, r>(x + c * r);
         twiddle<S, false>(x, tw, t);
         if constexpr (S + 1 < NS) {
+            void *buf = xp.next();
             store<S>(x, buf, t);
             team_sync(bar_id, NT);
             load<S + 1>(x, buf, t);
-            team_sync(bar_id, NT);
-            forward_from<S + 1>(x, buf, tw, t, bar_id);
+            forward_from<S + 1>(x, xp, tw, t, bar_id);
         }
     }
 
     template <int S>
-    __device__ static __forceinline__ void inverse_from(cplx<T> *x, void *buf, const cplx<T> *tw, int t, int bar_id) {
+    __device__ static __forceinline__ void inverse_from(cplx<T> *x, ExchPair &xp, const cplx<T> *tw, int t, int bar_id) {
         constexpr int r = Stage<M, S>::r;
         twiddle<S, true>(x, tw, t);
 #pragma unroll
         for (int c = 0; c < R / r; c++) dft<T, true, r>(x + c * r);
         if constexpr (S > 0) {
+            void *buf = xp.next();
             store<S>(x, buf, t);
             team_sync(bar_id, NT);
             load<S - 1>(x, buf, t);
-            team_sync(bar_id, NT);
-            inverse_from<S - 1>(x, buf, tw, t, bar_id);
+            inverse_from<S - 1>(x, xp, tw, t, bar_id);
         }
     }
 
     // Folded negacyclic transform.  In: x[n2] = a_j - i a_{j+M} for j = t + NT*n2 (no twist applied).
     // Out: the M evaluation points in slot order.
-    __device__ static __forceinline__ void forward(cplx<T> *x, void *buf, const cplx<T> *tw, int t, int bar_id) {
+    __device__ static __forceinline__ void forward(cplx<T> *x, ExchPair &xp, const cplx<T> *tw, int t, int bar_id) {
         fold_consts<false>(x);
-        forward_from<0>(x, buf, tw, t, bar_id);
+        forward_from<0>(x, xp, tw, t, bar_id);
     }
     // Slot order in -> x[n2] = M * (c_j - i c_{j+M}), j = t + NT*n2 (twist removed).
-    __device__ static __forceinline__ void inverse(cplx<T> *x, void *buf, const cplx<T> *tw, int t, int bar_id) {
-        inverse_from<NS - 1>(x, buf, tw, t, bar_id);
+    __device__ static __forceinline__ void inverse(cplx<T> *x, ExchPair &xp, const cplx<T> *tw, int t, int bar_id) {
+        inverse_from<NS - 1>(x, xp, tw, t, bar_id);
         fold_consts<true>(x);
     }
 };
