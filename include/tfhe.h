@@ -154,6 +154,26 @@ TFHE_B200_EXPORT void bootsNAND_batch(LweSample *results, const LweSample *a, co
 TFHE_B200_EXPORT void bootsMUX_batch(LweSample *results, const LweSample *a, const LweSample *b, const LweSample *c,
                                      int32_t count, const TFheGateBootstrappingCloudKeySet *bk);
 
+/* ---- tfhe.h:38-39: coefficient-domain bootstrap (same GPU path as the _FFT forms) ------------ */
+TFHE_B200_EXPORT void tfhe_bootstrap(LweSample *result, const LweBootstrappingKey *bk, Torus32 mu, const LweSample *x);
+TFHE_B200_EXPORT void tfhe_bootstrap_woKS(LweSample *result, const LweBootstrappingKey *bk, Torus32 mu,
+                                          const LweSample *x);
+
+/* ---- lwe-functions.h:25-68 and numeric-functions.h (approxPhase): host-side LWE helpers ------- */
+TFHE_B200_EXPORT void lweSymEncrypt(LweSample *result, Torus32 message, double alpha, const LweKey *key);
+TFHE_B200_EXPORT void lweSymEncryptWithExternalNoise(LweSample *result, Torus32 message, double noise, double alpha,
+                                                     const LweKey *key);
+TFHE_B200_EXPORT Torus32 lweSymDecrypt(const LweSample *sample, const LweKey *key, const int32_t Msize);
+TFHE_B200_EXPORT Torus32 approxPhase(Torus32 phase, int32_t Msize);
+TFHE_B200_EXPORT void lweClear(LweSample *result, const LweParams *params);
+TFHE_B200_EXPORT void lweCopy(LweSample *result, const LweSample *sample, const LweParams *params);
+TFHE_B200_EXPORT void lweNegate(LweSample *result, const LweSample *sample, const LweParams *params);
+TFHE_B200_EXPORT void lweNoiselessTrivial(LweSample *result, Torus32 mu, const LweParams *params);
+TFHE_B200_EXPORT void lweAddTo(LweSample *result, const LweSample *sample, const LweParams *params);
+TFHE_B200_EXPORT void lweSubTo(LweSample *result, const LweSample *sample, const LweParams *params);
+TFHE_B200_EXPORT void lweAddMulTo(LweSample *result, int32_t p, const LweSample *sample, const LweParams *params);
+TFHE_B200_EXPORT void lweSubMulTo(LweSample *result, int32_t p, const LweSample *sample, const LweParams *params);
+
 /* ---- tfhe_io.h: files in the reference's format (tfhe_io.cpp:90-136, 1010-1220) -------------
  * Same layout byte for byte, so key sets and ciphertexts move between this library and tfhe. */
 TFHE_B200_EXPORT void export_lweSample_toFile(FILE *F, const LweSample *lwesample, const LweParams *params);

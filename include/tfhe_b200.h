@@ -124,13 +124,30 @@ tfheb_status tfheb_encrypt(const tfheb_secret_key *sk, const int32_t *bits, int3
 tfheb_status tfheb_decrypt(const tfheb_secret_key *sk, const int32_t *cts, int32_t count, int32_t *bits,
                            int32_t *phases);
 
+/* Replaces lweSymEncrypt / lweSymDecrypt (lwe-functions.cpp:33-44, 86-90) for batches: torus
+ * messages mu[count] -> [count][n+1] with noise stdev `stdev`; decryption returns each phase
+ * rounded to the nearest multiple of 1/msize (approxPhase, numeric-functions.cpp:45-53). */
+tfheb_status tfheb_encrypt_torus(const tfheb_secret_key *sk, const int32_t *mu, int32_t count, double stdev,
+                                 uint64_t seed, int32_t *out);
+tfheb_status tfheb_decrypt_torus(const tfheb_secret_key *sk, const int32_t *cts, int32_t count, int32_t msize,
+                                 int32_t *out);
+
 /* Moves the cloud key to a GPU: FFT-domain bootstrapping key in the requested precisions
- * (bit 0 = FP64, bit 1 = split FP32), keyswitching key, twiddle tables.  The host-side FP64
- * transform replaces init_LweBootstrappingKeyFFT (lwe-bootstrapping-functions-fft.cpp:23-52).
+ * (bit 0 = FP64, bit 1 = split FP32), keyswitching key, twiddle tables.  The FFT-domain key is
+ * computed on the GPU with FP64 transforms, replacing init_LweBootstrappingKeyFFT
+ * (lwe-bootstrapping-functions-fft.cpp:23-52).
  * split_shift: weight 2^split_shift of the high limb in split mode (0 = the parameter-dependent
  * default of tfheb_default_split_shift). */
 tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *ck, int32_t device, int32_t precision_mask,
                                        int32_t split_shift);
+
+/* Copies the device FFT-domain bootstrapping key of `precision` to host memory (`bytes` must be
+ * n*(k+1)*l*(k+1)*N/2*16).  Per key polynomial, spectrum / M in slot order (tfheb_fft_slot_order):
+ *   FP64:  [8][N/16] double2 (re, im)
+ *   split: [4][2][N/16] float4 {re(2m), re(2m+1), im(2m), im(2m+1)} for register pair m and limb
+ *          (0 = hi, 1 = lo of c = hi * 2^S + lo).
+ * For tests and tooling; no reference counterpart. */
+tfheb_status tfheb_cloud_key_fft_download(const tfheb_cloud_key *ck, int32_t precision, void *out, size_t bytes);
 
 /* Batched gates on host buffers ([count][n+1] each; c only for MUX, b unused for NOT/COPY):
  * the batched counterpart of bootsNAND...bootsMUX (boot-gates.cpp:34-370).  Synchronous. */

@@ -78,6 +78,7 @@ def lib():
         L.tfheb_set_keyswitch_kernel.argtypes = [_V, _I32]
         L.tfheb_cloud_key_params.argtypes = [_V, ctypes.POINTER(Params)]
         L.tfheb_gate_batch_multi.argtypes = [_V, _I32, _I32, _I32, _I32, _V, _V, _V, _V]
+        L.tfheb_cloud_key_fft_download.argtypes = [_V, _I32, _V, ctypes.c_size_t]
         _C = ctypes.c_char_p
         L.tfheb_params_save.argtypes = [_C, ctypes.POINTER(Params)]
         L.tfheb_params_load.argtypes = [_C, ctypes.POINTER(Params)]
@@ -194,6 +195,19 @@ class CloudKey:
         ksk = np.zeros((p.k * p.N, p.ks_t, 1 << p.ks_basebit, p.n + 1), np.int32)
         _check(lib().tfheb_cloud_key_export(self.h, _p(bsk), _p(ksk)), "export")
         return bsk, ksk
+
+    def fft_key(self, precision):
+        """The device FFT-domain bootstrapping key as stored (tfheb_cloud_key_fft_download)."""
+        p = self.params
+        polys = p.n * (p.k + 1) * p.l * (p.k + 1)
+        nt = p.N // 16
+        if precision == FP64:
+            out = np.zeros((polys, 8, nt, 2), np.float64)
+        else:
+            out = np.zeros((polys, 4, 2, nt, 4), np.float32)
+        _check(lib().tfheb_cloud_key_fft_download(self.h, precision, _p(out), out.nbytes),
+               "tfheb_cloud_key_fft_download")
+        return out
 
     def to_device(self, device=0, precisions=(FP64, SPLIT_FP32), split_shift=0):
         mask = 0

@@ -354,6 +354,100 @@ void tfhe_bootstrap_woKS_FFT(LweSample *result, const LweBootstrappingKeyFFT *bk
     bootstrap_one(result, bk, mu, x, false);
 }
 
+// The coefficient-domain entry points (lwe-bootstrapping-functions.cpp:138-179) run the same GPU
+// path on the same key: the reference computes their external products exactly with integer
+// polynomial products, this library through its FFT (FP64 by default), so a result may differ
+// from the reference's by a few Torus32 units while decrypting the same.
+static void bootstrap_coef(LweSample *result, const LweBootstrappingKey *bk, Torus32 mu, const LweSample *x,
+                           bool with_ks) {
+    if (!bk || !bk->ck) die("bootstrapping key is empty");
+    tfheb_params p;
+    tfheb_cloud_key_params(bk->ck, &p);
+    const LweBootstrappingKeyFFT view{bk->ck, p.n, p.k * p.N, 0};  // moves missing device keys once
+    bootstrap_one(result, &view, mu, x, with_ks);
+}
+
+void tfhe_bootstrap(LweSample *result, const LweBootstrappingKey *bk, Torus32 mu, const LweSample *x) {
+    bootstrap_coef(result, bk, mu, x, true);
+}
+
+void tfhe_bootstrap_woKS(LweSample *result, const LweBootstrappingKey *bk, Torus32 mu, const LweSample *x) {
+    bootstrap_coef(result, bk, mu, x, false);
+}
+
+// ---- LWE helpers of lwe-functions.h (lwe-functions.cpp:33-178), host side -------------------
+
+void lweSymEncrypt(LweSample *result, Torus32 message, double alpha, const LweKey *key) {
+    const int32_t n = key->params->n;
+    std::vector<int32_t> ct(n + 1);
+    tfheb::encrypt_torus(n, key->key, &message, 1, alpha, next_seed(), ct.data());
+    std::memcpy(result->a, ct.data(), sizeof(int32_t) * n);
+    result->b = ct[n];
+    result->current_variance = alpha * alpha;
+}
+
+void lweSymEncryptWithExternalNoise(LweSample *result, Torus32 message, double noise, double alpha,
+                                    const LweKey *key) {
+    const int32_t n = key->params->n;
+    const Torus32 mu = (Torus32)((uint32_t)message + (uint32_t)tfheb::double_to_torus32(noise));
+    std::vector<int32_t> ct(n + 1);
+    tfheb::encrypt_torus(n, key->key, &mu, 1, 0.0, next_seed(), ct.data());
+    std::memcpy(result->a, ct.data(), sizeof(int32_t) * n);
+    result->b = ct[n];
+    result->current_variance = alpha * alpha;
+}
+
+Torus32 approxPhase(Torus32 phase, int32_t Msize) { return tfheb::approx_phase(phase, Msize); }
+
+Torus32 lweSymDecrypt(const LweSample *sample, const LweKey *key, const int32_t Msize) {
+    return tfheb::approx_phase(lwePhase(sample, key), Msize);
+}
+
+void lweClear(LweSample *result, const LweParams *params) {
+    std::memset(result->a, 0, sizeof(int32_t) * params->n);
+    result->b = 0;
+    result->current_variance = 0.;
+}
+
+void lweCopy(LweSample *result, const LweSample *sample, const LweParams *params) {
+    std::memmove(result->a, sample->a, sizeof(int32_t) * params->n);
+    result->b = sample->b;
+    result->current_variance = sample->current_variance;
+}
+
+void lweNegate(LweSample *result, const LweSample *sample, const LweParams *params) {
+    for (int32_t i = 0; i < params->n; i++) result->a[i] = (int32_t)(0u - (uint32_t)sample->a[i]);
+    result->b = (int32_t)(0u - (uint32_t)sample->b);
+    result->current_variance = sample->current_variance;
+}
+
+void lweNoiselessTrivial(LweSample *result, Torus32 mu, const LweParams *params) {
+    std::memset(result->a, 0, sizeof(int32_t) * params->n);
+    result->b = mu;
+    result->current_variance = 0.;
+}
+
+// result += p * sample (p = 1, -1 for lweAddTo / lweSubTo), variance += p^2 * variance
+static void lwe_add_mul(LweSample *result, int32_t p, const LweSample *sample, const LweParams *params) {
+    for (int32_t i = 0; i < params->n; i++)
+        result->a[i] = (int32_t)((uint32_t)result->a[i] + (uint32_t)p * (uint32_t)sample->a[i]);
+    result->b = (int32_t)((uint32_t)result->b + (uint32_t)p * (uint32_t)sample->b);
+    result->current_variance += (double)p * (double)p * sample->current_variance;
+}
+
+void lweAddTo(LweSample *result, const LweSample *sample, const LweParams *params) {
+    lwe_add_mul(result, 1, sample, params);
+}
+void lweSubTo(LweSample *result, const LweSample *sample, const LweParams *params) {
+    lwe_add_mul(result, -1, sample, params);
+}
+void lweAddMulTo(LweSample *result, int32_t p, const LweSample *sample, const LweParams *params) {
+    lwe_add_mul(result, p, sample, params);
+}
+void lweSubMulTo(LweSample *result, int32_t p, const LweSample *sample, const LweParams *params) {
+    lwe_add_mul(result, -p, sample, params);
+}
+
 }  // extern "C"
 
 // ================================================================================================

@@ -321,6 +321,21 @@ tfheb_status tfheb_encrypt(const tfheb_secret_key *sk, const int32_t *bits, int3
     return TFHEB_OK;
 }
 
+tfheb_status tfheb_encrypt_torus(const tfheb_secret_key *sk, const int32_t *mu, int32_t count, double stdev,
+                                 uint64_t seed, int32_t *out) {
+    if (!sk || count < 0 || (count > 0 && (!mu || !out)) || !(stdev >= 0)) return TFHEB_ERR_INVALID;
+    encrypt_torus(sk->sk.p.n, sk->sk.lwe_key.data(), mu, count, stdev, seed, out);
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_decrypt_torus(const tfheb_secret_key *sk, const int32_t *cts, int32_t count, int32_t msize,
+                                 int32_t *out) {
+    if (!sk || count < 0 || (count > 0 && (!cts || !out)) || msize < 1) return TFHEB_ERR_INVALID;
+    const int n = sk->sk.p.n;
+    for (int g = 0; g < count; g++) out[g] = approx_phase(phase(sk->sk, cts + (size_t)g * (n + 1)), msize);
+    return TFHEB_OK;
+}
+
 tfheb_status tfheb_decrypt(const tfheb_secret_key *sk, const int32_t *cts, int32_t count, int32_t *bits,
                            int32_t *phases) {
     if (!sk || !cts || count < 0) return TFHEB_ERR_INVALID;
@@ -362,6 +377,15 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32
     TFHEB_CUDA(upload_keyswitch_key(ck));
     std::vector<double> tab;
     build_tables_fp64(p.N, tab);
+    // the FFT-domain keys are computed on the device (key_transform.cu) from the coefficient key
+    // and the FP64 tables, both staged in temporary device buffers freed on every return path
+    struct Temp {
+        void *p = nullptr;
+        ~Temp() {
+            if (p) cudaFree(p);
+        }
+    } d_coef, d_tab64;
+    const size_t polys = (size_t)p.n * (p.k + 1) * p.l * (p.k + 1);
     for (int prec = 0; prec < 2; prec++) {
         if (!(precision_mask & (1 << prec))) continue;
         DeviceBsk &d = ck.dbsk[prec];
@@ -371,12 +395,18 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32
             cudaFree(d.tables);
             d.bsk = d.tables = nullptr;
         }
-        std::vector<uint8_t> fbsk;
-        transform_bsk(p, ck.bsk_coef.data(), prec, split_shift, fbsk);
-        TFHEB_CUDA(cudaMalloc(&d.bsk, fbsk.size()));
-        TFHEB_CUDA(cudaMemcpy(d.bsk, fbsk.data(), fbsk.size(), cudaMemcpyHostToDevice));
-        d.bsk_bytes = fbsk.size();
+        if (!d_coef.p) {
+            TFHEB_CUDA(cudaMalloc(&d_coef.p, ck.bsk_coef.size() * sizeof(int32_t)));
+            TFHEB_CUDA(cudaMemcpy(d_coef.p, ck.bsk_coef.data(), ck.bsk_coef.size() * sizeof(int32_t),
+                                  cudaMemcpyHostToDevice));
+            TFHEB_CUDA(cudaMalloc(&d_tab64.p, tab.size() * sizeof(double)));
+            TFHEB_CUDA(cudaMemcpy(d_tab64.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+        }
+        d.bsk_bytes = polys * (size_t)(p.N / 2) * 16;
+        TFHEB_CUDA(cudaMalloc(&d.bsk, d.bsk_bytes));
         d.split_shift = prec == TFHEB_SPLIT_FP32 ? split_shift : 0;
+        TFHEB_CUDA(launch_bsk_to_fft(p, prec, static_cast<const int32_t *>(d_coef.p),
+                                     static_cast<const double *>(d_tab64.p), d.bsk, split_shift, ck.stream));
         if (prec == TFHEB_FP64) {
             TFHEB_CUDA(cudaMalloc(&d.tables, tab.size() * sizeof(double)));
             TFHEB_CUDA(cudaMemcpy(d.tables, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -386,6 +416,24 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32
             TFHEB_CUDA(cudaMemcpy(d.tables, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice));
         }
     }
+    TFHEB_CUDA(cudaStreamSynchronize(ck.stream));
+    return TFHEB_OK;
+}
+
+/* Inspection of the device FFT-domain key (layouts in key_transform.cu). */
+tfheb_status tfheb_cloud_key_fft_download(const tfheb_cloud_key *c, int32_t precision, void *out, size_t bytes) {
+    if (!c || !out || (precision != TFHEB_FP64 && precision != TFHEB_SPLIT_FP32)) return TFHEB_ERR_INVALID;
+    const DeviceBsk &d = c->ck.dbsk[precision];
+    if (!d.bsk) {
+        set_error("tfheb_cloud_key_fft_download: no FFT-domain key of that precision on the device");
+        return TFHEB_ERR_INVALID;
+    }
+    if (bytes != d.bsk_bytes) {
+        set_error("tfheb_cloud_key_fft_download: buffer size must be " + std::to_string(d.bsk_bytes) + " bytes");
+        return TFHEB_ERR_INVALID;
+    }
+    TFHEB_CUDA(cudaSetDevice(c->ck.device));
+    TFHEB_CUDA(cudaMemcpy(out, d.bsk, bytes, cudaMemcpyDeviceToHost));
     return TFHEB_OK;
 }
 

@@ -1,5 +1,6 @@
-// host_keys.cu -- host-side key material: generation, encryption, and the FFT-domain
-// bootstrapping key in the kernels' slot layout.
+// host_keys.cu -- host-side key material: generation, encryption, the FFT twiddle tables and the
+// slot order of the kernels' spectra (the FFT-domain key itself is computed on the GPU,
+// key_transform.cu).
 //
 // Key generation follows the reference's distributions and structure
 //   lweKeyGen / tLweKeyGen            lwe-functions.cpp:20-26, tlwe-functions.cpp:15-23
@@ -11,7 +12,6 @@
 #include <atomic>
 #include <cmath>
 #include <functional>
-#include <complex>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -34,9 +34,17 @@ int32_t modswitch_from_torus32(int32_t phase, int32_t msize) {
     return (int32_t)(phase64 / interv);
 }
 
-static int32_t double_to_torus32(double d) {
+int32_t double_to_torus32(double d) {
     const double frac = d - (double)(int64_t)d;
     return (int32_t)(uint32_t)(uint64_t)(int64_t)(frac * 4294967296.0);
+}
+
+// the nearest multiple of 1/msize (approxPhase, numeric-functions.cpp:45-53)
+int32_t approx_phase(int32_t phase, int32_t msize) {
+    const uint64_t interv = ((UINT64_C(1) << 63) / (uint64_t)msize) * 2;
+    uint64_t p64 = ((uint64_t)(uint32_t)phase << 32) + interv / 2;
+    p64 -= p64 % interv;
+    return (int32_t)(uint32_t)(p64 >> 32);
 }
 
 // ---- generator -------------------------------------------------------------------------------
@@ -180,6 +188,21 @@ void encrypt(const SecretKey &sk, const int32_t *bits, int32_t count, uint64_t s
     }
 }
 
+// LWE encryptions of torus messages under key[n] with noise stdev (lweSymEncrypt, lwe-functions.cpp:33-44)
+void encrypt_torus(int n, const int32_t *key, const int32_t *mu, int32_t count, double stdev, uint64_t seed,
+                   int32_t *out) {
+    Rng rng(seed);
+    for (int g = 0; g < count; g++) {
+        int32_t *ct = out + (size_t)g * (n + 1);
+        uint32_t b = (uint32_t)mu[g] + (uint32_t)double_to_torus32(rng.normal() * stdev);
+        for (int i = 0; i < n; i++) {
+            ct[i] = rng.torus();
+            b += (uint32_t)ct[i] * (uint32_t)key[i];
+        }
+        ct[n] = (int32_t)b;
+    }
+}
+
 int32_t phase(const SecretKey &sk, const int32_t *ct) {
     uint32_t axs = 0;
     for (int i = 0; i < sk.p.n; i++) axs += (uint32_t)ct[i] * (uint32_t)sk.lwe_key[i];
@@ -237,37 +260,6 @@ void tables_m(std::vector<double> &tab) {
     }
 }
 
-using cd = std::complex<double>;
-
-// size-M complex DFT, W = exp(-2 pi i / M), natural order (iterative radix-2)
-struct HostFft {
-    int M;
-    std::vector<cd> w;
-    std::vector<int> rev;
-    explicit HostFft(int M_) : M(M_), w(M_ / 2), rev(M_) {
-        for (int i = 0; i < M / 2; i++)
-            w[i] = cd((double)std::cos(-2.0L * M_PI * i / M), (double)std::sin(-2.0L * M_PI * i / M));
-        int lg = 0;
-        while ((1 << lg) < M) lg++;
-        for (int i = 0; i < M; i++) {
-            int r = 0;
-            for (int b = 0; b < lg; b++)
-                if (i >> b & 1) r |= 1 << (lg - 1 - b);
-            rev[i] = r;
-        }
-    }
-    void run(std::vector<cd> &a) const {
-        for (int i = 0; i < M; i++)
-            if (i < rev[i]) std::swap(a[i], a[rev[i]]);
-        for (int len = 2; len <= M; len <<= 1)
-            for (int i = 0; i < M; i += len)
-                for (int j = 0; j < len / 2; j++) {
-                    const cd u = a[i + j], v = a[i + j + len / 2] * w[(size_t)j * (M / len)];
-                    a[i + j] = u + v;
-                    a[i + j + len / 2] = u - v;
-                }
-    }
-};
 }  // namespace
 
 void fill_slot_freq(int N, std::vector<int32_t> &sf) {
@@ -288,70 +280,6 @@ void build_tables_fp64(int N, std::vector<double> &tab) {
         case 1024: tables_m<1024>(tab); break;
         default: tab.clear();
     }
-}
-
-// bsk_coef [n][kpl][k+1][N] -> FFT domain, slot layout [n][kpl][k+1][R][NT], 16 bytes per slot:
-//   FP64: double2 (re, im) of B_k / M at [R][NT];
-//   split FP32: per register pair (2m, 2m+1) and limb, float4 {re, re', im, im'} of B_k / M at [4][2][NT]
-void transform_bsk(const tfheb_params &p, const int32_t *bsk_coef, int precision, int split_shift,
-                   std::vector<uint8_t> &out) {
-    const int N = p.N, M = N / 2, NT = M / kR, kpl = (p.k + 1) * p.l;
-    const size_t polys = (size_t)p.n * kpl * (p.k + 1);
-    out.assign(polys * M * 16, 0);
-    std::vector<int32_t> sf;
-    fill_slot_freq(N, sf);
-    const HostFft fft(M);
-    std::vector<cd> twist(M);
-    for (int j = 0; j < M; j++)
-        twist[j] = cd((double)std::cos(-M_PI * (long double)j / N), (double)std::sin(-M_PI * (long double)j / N));
-    const double scale = 1.0 / M;
-    auto fold_fft = [&](const int64_t *c, std::vector<cd> &z) {
-        for (int j = 0; j < M; j++) z[j] = cd((double)c[j], -(double)c[j + M]) * twist[j];
-        fft.run(z);
-    };
-    parallel_for((int)((polys + 63) / 64), [&](int chunk) {
-        std::vector<cd> zh(M), zl(M);
-        std::vector<int64_t> hi(N), lo(N);
-        for (size_t poly = (size_t)chunk * 64; poly < std::min(polys, (size_t)chunk * 64 + 64); poly++) {
-            const int32_t *c = bsk_coef + poly * N;
-            uint8_t *dst = out.data() + poly * M * 16;
-            if (precision == TFHEB_FP64) {
-                for (int j = 0; j < N; j++) hi[j] = c[j];
-                fold_fft(hi.data(), zh);
-                double *d = reinterpret_cast<double *>(dst);
-                for (int s = 0; s < kR * NT; s++) {
-                    const cd v = zh[sf[s]] * scale;
-                    d[2 * s] = v.real();
-                    d[2 * s + 1] = v.imag();
-                }
-            } else {
-                // c = hi * 2^S + lo, lo in [-2^(S-1), 2^(S-1))  (exact in int64, reduced mod 2^32 later)
-                const int S = split_shift;
-                for (int j = 0; j < N; j++) {
-                    const int64_t v = c[j];
-                    const int64_t l = ((v + ((int64_t)1 << (S - 1))) & (((int64_t)1 << S) - 1)) - ((int64_t)1 << (S - 1));
-                    lo[j] = l;
-                    hi[j] = (v - l) >> S;
-                }
-                fold_fft(hi.data(), zh);
-                fold_fft(lo.data(), zl);
-                // [m < 4][limb: hi, lo][t] x float4 {re(r), re(r+1), im(r), im(r+1)}, r = 2m: the
-                // register pairs of the packed multiply-accumulate
-                float *d = reinterpret_cast<float *>(dst);
-                for (int r = 0; r < kR; r++)
-                    for (int t = 0; t < NT; t++) {
-                        const int s = r * NT + t, m = r >> 1, odd = r & 1;
-                        const cd h = zh[sf[s]] * scale, l = zl[sf[s]] * scale;
-                        float *eh = d + ((size_t)(m * 2 + 0) * NT + t) * 4;
-                        float *el = d + ((size_t)(m * 2 + 1) * NT + t) * 4;
-                        eh[odd] = (float)h.real();
-                        eh[2 + odd] = (float)h.imag();
-                        el[odd] = (float)l.real();
-                        el[2 + odd] = (float)l.imag();
-                    }
-            }
-        }
-    });
 }
 
 }  // namespace tfheb

@@ -115,14 +115,20 @@ struct SecretKey {
 void keygen(const tfheb_params &p, uint64_t seed, SecretKey &sk, CloudKey &ck);
 void encrypt(const SecretKey &sk, const int32_t *bits, int32_t count, uint64_t seed, int32_t *out);
 int32_t phase(const SecretKey &sk, const int32_t *ct);
+void encrypt_torus(int n, const int32_t *key, const int32_t *mu, int32_t count, double stdev, uint64_t seed,
+                   int32_t *out);
+int32_t double_to_torus32(double d);
+int32_t approx_phase(int32_t phase, int32_t msize);
 int32_t modswitch_to_torus32(int32_t mu, int32_t msize);
 int32_t modswitch_from_torus32(int32_t phase, int32_t msize);
 
 // FFT-domain key preparation (host FP64), layout-compatible with the kernels.
 void build_tables_fp64(int N, std::vector<double> &tables);  // complex pairs (re,im)
 void fill_slot_freq(int N, std::vector<int32_t> &slot_freq); // [R][NT] -> frequency index
-void transform_bsk(const tfheb_params &p, const int32_t *bsk_coef, int precision, int split_shift,
-                   std::vector<uint8_t> &out);
+// key_transform.cu: coefficient-domain bootstrapping key [n][kpl][k+1][N] on the device -> the
+// FFT-domain layout of `precision` (d_out: n*kpl*(k+1)*N/2*16 bytes), on stream s.
+cudaError_t launch_bsk_to_fft(const tfheb_params &p, int precision, const int32_t *d_coef, const double *d_tables64,
+                              void *d_out, int split_shift, cudaStream_t s);
 
 // ---- kernel launchers (kernels.cu) ----------------------------------------------------------
 cudaError_t launch_prologue(const tfheb_params &p, const BootDesc *d_desc, int boots, const int32_t *a,
