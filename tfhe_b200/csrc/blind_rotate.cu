@@ -82,7 +82,11 @@ struct BrLayout {
     static constexpr size_t teams = tables + tables_bytes;
     static constexpr size_t team_acc = 4 * (size_t)KP1 * N;
     static constexpr size_t team_xbuf = ((size_t)Exch<T, M>::bytes + 15) / 16 * 16;  // one exchange buffer
-    static constexpr size_t team_buf = 2 * team_xbuf;                                // the alternating pair
+    // two alternating exchange buffers (one barrier per exchange) up to N = 1024; at N = 2048 the
+    // second buffer costs more in shared memory and register pressure than the barrier it saves
+    // (measured 78.3 vs 72.6 ms per 2048 split bootstraps)
+    static constexpr int xbufs = N >= 2048 ? 1 : 2;
+    static constexpr size_t team_buf = xbufs * team_xbuf;
     __host__ __device__ static size_t team_bytes(int nsteps) {
         return team_acc + team_buf + 16 * (((size_t)nsteps + 4 + 3) / 4);
     }
@@ -181,7 +185,7 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
 
     unsigned char *tb = smem + Lay::teams + (size_t)team * Lay::team_bytes(args.nsteps);
     uint32_t *s_acc = reinterpret_cast<uint32_t *>(tb);
-    ExchPair xp{tb + Lay::team_acc, (uint32_t)Lay::team_xbuf, 0u};
+    ExchPair xp{tb + Lay::team_acc, Lay::xbufs == 2 ? (uint32_t)Lay::team_xbuf : 0u, 0u};
     int32_t *s_bara = reinterpret_cast<int32_t *>(tb + Lay::team_acc + Lay::team_buf);
     const cplx<T> *s_tw = s_tab;
 

@@ -257,12 +257,14 @@ __device__ __forceinline__ void team_sync(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Two exchange buffers of a team, used alternately by consecutive exchanges (the parity runs on
-// across transforms).  Exchange k stores into buffer k % 2, whose last readers (exchange k-2) all
-// passed the barrier of exchange k-1 before this store: one barrier per exchange suffices.
+// Exchange buffers of a team.  With two (stride = bytes of one buffer) consecutive exchanges
+// alternate between them (the parity runs on across transforms): exchange k stores into buffer
+// k % 2, whose last readers (exchange k-2) all passed the barrier of exchange k-1 before this store,
+// so one barrier per exchange suffices.  With one (stride = 0) every exchange ends with a second
+// barrier before the buffer is reused; variants short of shared memory or registers use that.
 struct ExchPair {
     unsigned char *base;
-    uint32_t stride;  // bytes of one buffer
+    uint32_t stride;  // bytes of one buffer; 0: a single buffer
     uint32_t parity;  // buffer of the next exchange
     __device__ __forceinline__ void *next() {
         void *b = base + parity * stride;
@@ -271,7 +273,7 @@ struct ExchPair {
     }
 };
 
-// Team FFT: T = M/R threads, t in [0,T), registers x[R], two exchange buffers (Exch<T, M>::bytes each).
+// Team FFT: T = M/R threads, t in [0,T), registers x[R], one or two exchange buffers (ExchPair).
 template <typename T, int M, int R>
 struct TeamFft {
     static constexpr int NT = M / R;  // threads per team
@@ -359,6 +361,7 @@ struct TeamFft {
             store<S>(x, buf, t);
             team_sync(bar_id, NT);
             load<S + 1>(x, buf, t);
+            if (xp.stride == 0) team_sync(bar_id, NT);
             forward_from<S + 1>(x, xp, tw, t, bar_id);
         }
     }
@@ -374,6 +377,7 @@ struct TeamFft {
             store<S>(x, buf, t);
             team_sync(bar_id, NT);
             load<S - 1>(x, buf, t);
+            if (xp.stride == 0) team_sync(bar_id, NT);
             inverse_from<S - 1>(x, xp, tw, t, bar_id);
         }
     }
