@@ -244,8 +244,10 @@ int32_t tfheb_default_split_shift(const tfheb_params *p);
  * calls (test-long-run.cpp:61-185, test-addition-boot.cpp).  Wires 0..num_inputs-1 are primary
  * inputs; gate g (codes as above, topological order) produces wire num_inputs+g and reads wires
  * in_a[g], in_b[g] (and in_c[g] for MUX; only in_a for NOT/COPY), each below num_inputs+g.
- * create: levels the gates, uploads per-level descriptors and allocates the scratch of the widest
- * level.  run: d_wires is a device array [num_inputs+num_gates][n+1] whose input rows the caller
+ * create: levels the gates (as many levels as the critical path; gates with slack move to levels
+ * where they complete blind-rotation waves, one schedule per precision for the key's current
+ * launch variants), uploads per-level descriptors and allocates the scratch of the widest level;
+ * info reports the level count and the widest level of the split-FP32 schedule.  run: d_wires is a device array [num_inputs+num_gates][n+1] whose input rows the caller
  * filled; on return (stream-ordered) row num_inputs+g holds gate g's output.  With use_graph, the
  * first run on a (precision, d_wires) pair evaluates eagerly and captures the level sequence into a
  * CUDA graph; later runs replay that graph with one launch. */

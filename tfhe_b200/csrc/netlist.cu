@@ -2,7 +2,9 @@
 //
 // The reference evaluates circuits one gate call at a time (e.g. test-long-run.cpp:61-185,
 // test-addition-boot.cpp); here the whole circuit is scheduled at creation:
-//   * each gate gets a level = 1 + the deepest level among its inputs (primary inputs are level 0);
+//   * each gate gets a level: the earliest is 1 + the deepest level among its inputs (primary inputs
+//     are level 0); gates with slack then move later to fill blind-rotation waves (pack_levels),
+//     keeping the number of levels at the critical path length;
 //   * gates are renumbered level by level into an internal wire array, bootstrapped gates first in
 //     each level, so a level's outputs are one contiguous block of rows;
 //   * per level, one launch sequence covers all its gates whatever their types: a prologue that reads
@@ -82,21 +84,37 @@ struct Level {
 }  // namespace
 }  // namespace tfheb
 
+namespace tfheb {
+namespace {
+// One level schedule of a netlist: levels, their descriptors and the internal row order.  Each
+// precision has its own, packed for the wave of that precision's blind-rotation variant.
+struct Schedule {
+    std::vector<Level> levels;
+    int max_boots = 0, max_gates = 0;
+    BootDescRows *d_boot = nullptr;
+    GateDesc *d_gate = nullptr;
+    UnaryDesc *d_unary = nullptr;
+    int32_t *d_out_perm = nullptr;  // internal gate row (minus num_inputs) -> user row
+    int graph_kernels = 0;          // kernels replayed by one graph launch
+    void release() {
+        cudaFree(d_boot);
+        cudaFree(d_gate);
+        cudaFree(d_unary);
+        cudaFree(d_out_perm);
+    }
+};
+}  // namespace
+}  // namespace tfheb
+
 struct tfheb_netlist {
     tfheb_cloud_key *ck = nullptr;
     int num_inputs = 0, num_gates = 0;
-    std::vector<tfheb::Level> levels;
-    int max_boots = 0, max_gates = 0;
-    // device state
-    tfheb::BootDescRows *d_boot = nullptr;
-    tfheb::GateDesc *d_gate = nullptr;
-    tfheb::UnaryDesc *d_unary = nullptr;
-    int32_t *d_out_perm = nullptr;  // internal gate row (minus num_inputs) -> user row
+    tfheb::Schedule sched[2];       // [TFHEB_FP64], [TFHEB_SPLIT_FP32]
+    // device state shared by both schedules
     int32_t *d_wires = nullptr;     // internal wire array [num_inputs + num_gates][n+1]
     int32_t *d_bara = nullptr, *d_acc = nullptr, *d_ksin = nullptr;
     std::map<std::pair<int, const int32_t *>, cudaGraphExec_t> graphs;
     std::map<std::pair<int, const int32_t *>, cudaGraph_t> graph_defs;
-    int graph_kernels = 0;  // kernels replayed by one graph launch
 };
 
 using namespace tfheb;
@@ -117,10 +135,11 @@ cudaError_t enqueue_netlist(tfheb_netlist *nl, CloudKey &ck, int precision, int3
     cudaError_t e = cudaMemcpyAsync(nl->d_wires, user_wires, (size_t)nl->num_inputs * n1 * 4,
                                     cudaMemcpyDeviceToDevice, s);
     int launches = 0;
-    for (const Level &L : nl->levels) {
+    const Schedule &sc = nl->sched[precision];
+    for (const Level &L : sc.levels) {
         if (e != cudaSuccess) break;
         if (L.boots > 0) {
-            prologue_rows_kernel<<<L.boots, 256, 0, s>>>(nl->d_boot + L.boot_off,
+            prologue_rows_kernel<<<L.boots, 256, 0, s>>>(sc.d_boot + L.boot_off,
                                                          reinterpret_cast<const uint32_t *>(nl->d_wires), p.n, interv,
                                                          nl->d_bara, bs);
             if ((e = cudaGetLastError()) != cudaSuccess) break;
@@ -128,21 +147,21 @@ cudaError_t enqueue_netlist(tfheb_netlist *nl, CloudKey &ck, int precision, int3
                                     modswitch_to_torus32(1, 8), nullptr, nl->d_acc, s, ck.d_err, ck.stall_producer,
                                     ck.wait_timeout_ns, ck.br_variant[precision]);
             if (e != cudaSuccess) break;
-            e = launch_extract(p, nl->d_gate + L.gate_off, L.gates, nl->d_acc, nl->d_ksin, kN1, s);
+            e = launch_extract(p, sc.d_gate + L.gate_off, L.gates, nl->d_acc, nl->d_ksin, kN1, s);
             if (e != cudaSuccess) break;
             e = launch_keyswitch(ck, L.gates, nl->d_ksin, kN1,
                                  nl->d_wires + (size_t)L.out_row * n1, s);
             launches += 4;
         }
         if (e == cudaSuccess && L.unaries > 0) {
-            unary_rows_kernel<<<L.unaries, 256, 0, s>>>(nl->d_unary + L.unary_off,
+            unary_rows_kernel<<<L.unaries, 256, 0, s>>>(sc.d_unary + L.unary_off,
                                                          reinterpret_cast<uint32_t *>(nl->d_wires), p.n);
             e = cudaGetLastError();
             launches += 1;
         }
     }
     if (e == cudaSuccess && nl->num_gates > 0) {
-        permute_rows_kernel<<<nl->num_gates, 256, 0, s>>>(nl->d_out_perm, reinterpret_cast<const uint32_t *>(nl->d_wires),
+        permute_rows_kernel<<<nl->num_gates, 256, 0, s>>>(sc.d_out_perm, reinterpret_cast<const uint32_t *>(nl->d_wires),
                                                           reinterpret_cast<uint32_t *>(user_wires), p.n, nl->num_inputs);
         e = cudaGetLastError();
         launches += 1;
@@ -151,35 +170,92 @@ cudaError_t enqueue_netlist(tfheb_netlist *nl, CloudKey &ck, int precision, int3
     return e;
 }
 
-}  // namespace
+// Bootstraps one blind-rotation launch runs per wave: SMs x bootstraps per CTA of the key's current
+// variant for `precision`.
+int wave_bootstraps(const CloudKey &ck, int precision) {
+    int sms = 0, G[16] = {0}, D[16] = {0};
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ck.device);
+    const int nv = br_variants(ck.p.N, precision, G, D, 16);
+    const int v = ck.br_variant[precision];
+    return std::max(1, sms) * (nv > 0 && v < nv ? G[v] : 1);
+}
 
-extern "C" {
-
-tfheb_status tfheb_netlist_create(tfheb_cloud_key *c, int32_t num_inputs, int32_t num_gates, const int32_t *gates,
-                                  const int32_t *in_a, const int32_t *in_b, const int32_t *in_c,
-                                  tfheb_netlist **out) {
-    if (!c || !out || num_inputs <= 0 || num_gates < 0 || (num_gates > 0 && (!gates || !in_a))) return TFHEB_ERR_INVALID;
-    std::lock_guard<std::mutex> lock(c->mu);
-    CloudKey &ck = c->ck;
-    if (ck.device < 0) return nl_fail("cloud key is not on a device (call tfheb_cloud_key_to_device)");
-    // levels
-    std::vector<int> level(num_inputs + num_gates, 0);
-    for (int g = 0; g < num_gates; g++) {
-        const int w = num_inputs + g, code = gates[g];
-        if (code < 0 || code > TFHEB_COPY) return nl_fail("netlist: unknown gate code at gate " + std::to_string(g));
-        const int nin = code == TFHEB_MUX ? 3 : (code >= TFHEB_NOT ? 1 : 2);
-        const int32_t *ins[3] = {in_a, in_b, in_c};
-        int lv = 0;
-        for (int k = 0; k < nin; k++) {
-            if (!ins[k]) return nl_fail("netlist: missing operand array");
-            const int src = ins[k][g];
-            if (src < 0 || src >= w) return nl_fail("netlist: gate " + std::to_string(g) + " reads a later wire");
-            lv = std::max(lv, level[src]);
+// Level assignment that fills blind-rotation waves.  `level` holds each gate's earliest level
+// (1 + its deepest input) on entry.  Every gate gets a deadline, its latest level that keeps the
+// number of levels at nlev (1 below the earliest deadline among its consumers; nlev without
+// consumers).  Level s then takes every ready gate whose deadline is s, and tops the level up with
+// other ready gates, earliest deadline first, while its bootstraps stay within the waves the
+// mandatory gates already start (a multiple of `wave`).  A gate is ready once all its inputs sit on
+// earlier levels, so the evaluation order stays valid; NOT/COPY gates (no bootstrap) go on the
+// first level where they are ready.
+void pack_levels(int num_inputs, int num_gates, const int32_t *gates, const int32_t *in_a, const int32_t *in_b,
+                 const int32_t *in_c, int nlev, int wave, std::vector<int> &level) {
+    if (num_gates == 0 || wave <= 1) return;
+    const int32_t *ins[3] = {in_a, in_b, in_c};
+    auto nin = [&](int g) { return gates[g] == TFHEB_MUX ? 3 : (gates[g] >= TFHEB_NOT ? 1 : 2); };
+    auto boots = [&](int g) { return gates[g] == TFHEB_MUX ? 2 : (gates[g] >= TFHEB_NOT ? 0 : 1); };
+    // deadlines, consumers first (a gate only reads earlier wires)
+    std::vector<int> deadline(num_gates, nlev);
+    for (int g = num_gates - 1; g >= 0; g--)
+        for (int k = 0; k < nin(g); k++) {
+            const int src = ins[k][g] - num_inputs;
+            if (src >= 0) deadline[src] = std::min(deadline[src], deadline[g] - 1);
         }
-        level[w] = lv + 1;
+    // consumer lists and unscheduled-input counts
+    std::vector<int> cons_off(num_gates + 1, 0), waiting(num_gates, 0);
+    for (int g = 0; g < num_gates; g++)
+        for (int k = 0; k < nin(g); k++) {
+            const int src = ins[k][g] - num_inputs;
+            if (src >= 0) cons_off[src + 1]++, waiting[g]++;
+        }
+    for (int g = 0; g < num_gates; g++) cons_off[g + 1] += cons_off[g];
+    std::vector<int> cons(cons_off[num_gates]), fill(cons_off.begin(), cons_off.end() - 1);
+    for (int g = 0; g < num_gates; g++)
+        for (int k = 0; k < nin(g); k++) {
+            const int src = ins[k][g] - num_inputs;
+            if (src >= 0) cons[fill[src]++] = g;
+        }
+    // ready gates bucketed by deadline; unary gates in their own list
+    std::vector<std::vector<int>> bucket(nlev + 2);
+    std::vector<size_t> head(nlev + 2, 0);
+    std::vector<int> unary_ready;
+    auto make_ready = [&](int g) {
+        if (boots(g) == 0) unary_ready.push_back(g);
+        else bucket[deadline[g]].push_back(g);
+    };
+    for (int g = 0; g < num_gates; g++)
+        if (waiting[g] == 0) make_ready(g);
+    std::vector<int> placed;
+    for (int s = 1; s <= nlev; s++) {
+        placed.clear();
+        std::vector<int> un;
+        un.swap(unary_ready);
+        for (int g : un) placed.push_back(g);
+        int used = 0;
+        for (; head[s] < bucket[s].size(); head[s]++) {  // mandatory: deadline s
+            const int g = bucket[s][head[s]];
+            placed.push_back(g);
+            used += boots(g);
+        }
+        const int cap = (std::max(used, 1) + wave - 1) / wave * wave;
+        for (int t = s + 1; t <= nlev && used < cap; t++)
+            for (; head[t] < bucket[t].size() && used + boots(bucket[t][head[t]]) <= cap; head[t]++) {
+                const int g = bucket[t][head[t]];
+                placed.push_back(g);
+                used += boots(g);
+            }
+        for (int g : placed) level[num_inputs + g] = s;
+        for (int g : placed)
+            for (int i = cons_off[g]; i < cons_off[g + 1]; i++)
+                if (--waiting[cons[i]] == 0) make_ready(cons[i]);
     }
-    const int nlev = num_gates ? *std::max_element(level.begin() + num_inputs, level.end()) : 0;
-    // internal order: by level, bootstrapped gates before NOT/COPY
+}
+
+// Internal order (by level, bootstrapped gates before NOT/COPY in each level), descriptors and the
+// output permutation of one level assignment, uploaded to the device.
+cudaError_t build_schedule(int num_inputs, int num_gates, const int32_t *gates,
+                           const int32_t *in_a, const int32_t *in_b, const int32_t *in_c, int nlev,
+                           const std::vector<int> &level, Schedule &sc) {
     std::vector<int> order(num_gates);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
@@ -193,10 +269,6 @@ tfheb_status tfheb_netlist_create(tfheb_cloud_key *c, int32_t num_inputs, int32_
         row_of[num_inputs + order[r]] = num_inputs + r;
         perm[r] = num_inputs + order[r];
     }
-    auto *nl = new tfheb_netlist();
-    nl->ck = c;
-    nl->num_inputs = num_inputs;
-    nl->num_gates = num_gates;
     std::vector<BootDescRows> bd;
     std::vector<GateDesc> gd;
     std::vector<UnaryDesc> ud;
@@ -228,33 +300,76 @@ tfheb_status tfheb_netlist_create(tfheb_cloud_key *c, int32_t num_inputs, int32_
         L.boots = (int)bd.size() - L.boot_off;
         L.gates = (int)gd.size() - L.gate_off;
         L.unaries = (int)ud.size() - L.unary_off;
-        nl->max_boots = std::max(nl->max_boots, L.boots);
-        nl->max_gates = std::max(nl->max_gates, L.gates);
-        nl->levels.push_back(L);
+        sc.max_boots = std::max(sc.max_boots, L.boots);
+        sc.max_gates = std::max(sc.max_gates, L.gates);
+        sc.levels.push_back(L);
+    }
+    auto alloc = [&](void **ptr, size_t bytes) { return bytes ? cudaMalloc(ptr, bytes) : cudaSuccess; };
+    cudaError_t e = alloc((void **)&sc.d_boot, bd.size() * sizeof(BootDescRows));
+    if (e == cudaSuccess) e = alloc((void **)&sc.d_gate, gd.size() * sizeof(GateDesc));
+    if (e == cudaSuccess) e = alloc((void **)&sc.d_unary, ud.size() * sizeof(UnaryDesc));
+    if (e == cudaSuccess) e = alloc((void **)&sc.d_out_perm, perm.size() * 4);
+    if (e == cudaSuccess && !bd.empty())
+        e = cudaMemcpy(sc.d_boot, bd.data(), bd.size() * sizeof(BootDescRows), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !gd.empty())
+        e = cudaMemcpy(sc.d_gate, gd.data(), gd.size() * sizeof(GateDesc), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !ud.empty())
+        e = cudaMemcpy(sc.d_unary, ud.data(), ud.size() * sizeof(UnaryDesc), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !perm.empty())
+        e = cudaMemcpy(sc.d_out_perm, perm.data(), perm.size() * 4, cudaMemcpyHostToDevice);
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+tfheb_status tfheb_netlist_create(tfheb_cloud_key *c, int32_t num_inputs, int32_t num_gates, const int32_t *gates,
+                                  const int32_t *in_a, const int32_t *in_b, const int32_t *in_c,
+                                  tfheb_netlist **out) {
+    if (!c || !out || num_inputs <= 0 || num_gates < 0 || (num_gates > 0 && (!gates || !in_a))) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    if (ck.device < 0) return nl_fail("cloud key is not on a device (call tfheb_cloud_key_to_device)");
+    // levels
+    std::vector<int> level(num_inputs + num_gates, 0);
+    for (int g = 0; g < num_gates; g++) {
+        const int w = num_inputs + g, code = gates[g];
+        if (code < 0 || code > TFHEB_COPY) return nl_fail("netlist: unknown gate code at gate " + std::to_string(g));
+        const int nin = code == TFHEB_MUX ? 3 : (code >= TFHEB_NOT ? 1 : 2);
+        const int32_t *ins[3] = {in_a, in_b, in_c};
+        int lv = 0;
+        for (int k = 0; k < nin; k++) {
+            if (!ins[k]) return nl_fail("netlist: missing operand array");
+            const int src = ins[k][g];
+            if (src < 0 || src >= w) return nl_fail("netlist: gate " + std::to_string(g) + " reads a later wire");
+            lv = std::max(lv, level[src]);
+        }
+        level[w] = lv + 1;
+    }
+    const int nlev = num_gates ? *std::max_element(level.begin() + num_inputs, level.end()) : 0;
+    auto *nl = new tfheb_netlist();
+    nl->ck = c;
+    nl->num_inputs = num_inputs;
+    nl->num_gates = num_gates;
+    cudaError_t e = cudaSetDevice(ck.device);
+    for (int prec = 0; prec < 2 && e == cudaSuccess; prec++) {
+        std::vector<int> lv(level);
+        pack_levels(num_inputs, num_gates, gates, in_a, in_b, in_c, nlev, wave_bootstraps(ck, prec), lv);
+        e = build_schedule(num_inputs, num_gates, gates, in_a, in_b, in_c, nlev, lv, nl->sched[prec]);
     }
     const tfheb_params &p = ck.p;
     const size_t rows = (size_t)num_inputs + num_gates;
+    const int max_boots = std::max(nl->sched[0].max_boots, nl->sched[1].max_boots);
+    const int max_gates = std::max(nl->sched[0].max_gates, nl->sched[1].max_gates);
     auto alloc = [&](void **ptr, size_t bytes) { return bytes ? cudaMalloc(ptr, bytes) : cudaSuccess; };
-    cudaError_t e = cudaSetDevice(ck.device);
-    if (e == cudaSuccess) e = alloc((void **)&nl->d_boot, bd.size() * sizeof(BootDescRows));
-    if (e == cudaSuccess) e = alloc((void **)&nl->d_gate, gd.size() * sizeof(GateDesc));
-    if (e == cudaSuccess) e = alloc((void **)&nl->d_unary, ud.size() * sizeof(UnaryDesc));
-    if (e == cudaSuccess) e = alloc((void **)&nl->d_out_perm, perm.size() * 4);
     if (e == cudaSuccess) e = alloc((void **)&nl->d_wires, rows * (p.n + 1) * 4);
-    if (e == cudaSuccess) e = alloc((void **)&nl->d_bara, (size_t)nl->max_boots * bara_stride_for(p) * 4);
-    if (e == cudaSuccess) e = alloc((void **)&nl->d_acc, (size_t)nl->max_boots * (p.k + 1) * p.N * 4);
-    if (e == cudaSuccess) e = alloc((void **)&nl->d_ksin, (size_t)nl->max_gates * (p.k * p.N + 1) * 4);
-    if (e == cudaSuccess && !bd.empty())
-        e = cudaMemcpy(nl->d_boot, bd.data(), bd.size() * sizeof(BootDescRows), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !gd.empty())
-        e = cudaMemcpy(nl->d_gate, gd.data(), gd.size() * sizeof(GateDesc), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !ud.empty())
-        e = cudaMemcpy(nl->d_unary, ud.data(), ud.size() * sizeof(UnaryDesc), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !perm.empty())
-        e = cudaMemcpy(nl->d_out_perm, perm.data(), perm.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = alloc((void **)&nl->d_bara, (size_t)max_boots * bara_stride_for(p) * 4);
+    if (e == cudaSuccess) e = alloc((void **)&nl->d_acc, (size_t)max_boots * (p.k + 1) * p.N * 4);
+    if (e == cudaSuccess) e = alloc((void **)&nl->d_ksin, (size_t)max_gates * (p.k * p.N + 1) * 4);
     if (e != cudaSuccess) {
         set_error(std::string("tfheb_netlist_create: ") + cudaGetErrorString(e));
-        delete nl;  // device buffers already allocated are released by the process teardown
+        tfheb_netlist_free(nl);
         return e == cudaErrorMemoryAllocation ? TFHEB_ERR_NOMEM : TFHEB_ERR_CUDA;
     }
     *out = nl;
@@ -263,10 +378,12 @@ tfheb_status tfheb_netlist_create(tfheb_cloud_key *c, int32_t num_inputs, int32_
 
 tfheb_status tfheb_netlist_info(const tfheb_netlist *nl, int32_t *num_levels, int32_t *max_width) {
     if (!nl) return TFHEB_ERR_INVALID;
-    if (num_levels) *num_levels = (int32_t)nl->levels.size();
+    // both schedules have the same number of levels; the widths are those of the split-FP32 one
+    const Schedule &sc = nl->sched[TFHEB_SPLIT_FP32];
+    if (num_levels) *num_levels = (int32_t)sc.levels.size();
     if (max_width) {
         int w = 0;
-        for (const auto &L : nl->levels) w = std::max(w, L.gates + L.unaries);
+        for (const auto &L : sc.levels) w = std::max(w, L.gates + L.unaries);
         *max_width = w;
     }
     return TFHEB_OK;
@@ -298,7 +415,7 @@ tfheb_status tfheb_netlist_run(tfheb_netlist *nl, int32_t precision, int32_t *d_
         cudaGraphExec_t ge = nullptr;
         if (e == cudaSuccess) e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            const cudaError_t e1 = enqueue_netlist(nl, ck, precision, d_wires, s, &nl->graph_kernels);
+            const cudaError_t e1 = enqueue_netlist(nl, ck, precision, d_wires, s, &nl->sched[precision].graph_kernels);
             const cudaError_t e2 = cudaStreamEndCapture(s, &g);
             e = e1 != cudaSuccess ? e1 : e2;
         }
@@ -313,7 +430,7 @@ tfheb_status tfheb_netlist_run(tfheb_netlist *nl, int32_t precision, int32_t *d_
     }
     const cudaError_t e = cudaGraphLaunch(it->second, s);
     if (e != cudaSuccess) return nl_fail(std::string("tfheb_netlist_run: ") + cudaGetErrorString(e), TFHEB_ERR_CUDA);
-    g_kernel_launches += nl->graph_kernels;
+    g_kernel_launches += nl->sched[precision].graph_kernels;
     return TFHEB_OK;
 }
 
@@ -322,10 +439,7 @@ void tfheb_netlist_free(tfheb_netlist *nl) {
     cudaSetDevice(nl->ck->ck.device);
     for (auto &kv : nl->graphs) cudaGraphExecDestroy(kv.second);
     for (auto &kv : nl->graph_defs) cudaGraphDestroy(kv.second);
-    cudaFree(nl->d_boot);
-    cudaFree(nl->d_gate);
-    cudaFree(nl->d_unary);
-    cudaFree(nl->d_out_perm);
+    for (auto &sc : nl->sched) sc.release();
     cudaFree(nl->d_wires);
     cudaFree(nl->d_bara);
     cudaFree(nl->d_acc);
