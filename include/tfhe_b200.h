@@ -204,8 +204,9 @@ tfheb_status tfheb_synchronize(tfheb_cloud_key *ck);
  * device waits; this is the failure-detection knob of the GPU engine. */
 tfheb_status tfheb_set_wait_timeout(tfheb_cloud_key *ck, uint64_t timeout_ns);
 
-/* Failure-detection test hook: when set, the blind rotation's key-streaming warp issues no copies,
- * so every consumer wait runs out after the timeout and the launch reports TFHEB_ERR_TIMEOUT with
+/* Failure-detection test hook: when set, the blind rotation's key-streaming warp and the
+ * keyswitch kernels' copy-issuing thread issue no copies, so every consumer wait runs out after the
+ * timeout and the launch reports TFHEB_ERR_TIMEOUT (from the call or from tfheb_synchronize) with
  * the context still usable.  No reference counterpart. */
 tfheb_status tfheb_test_stall_key_stream(tfheb_cloud_key *ck, int32_t stall);
 

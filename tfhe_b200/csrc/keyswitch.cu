@@ -121,7 +121,7 @@ template <int CW>
 __global__ void __launch_bounds__(kKsThreads, 2)
     keyswitch_tiled_kernel(const int32_t *__restrict__ tiles, const uint32_t *__restrict__ in, int in_stride,
                            uint32_t *__restrict__ out, int count, int n, int kN, int slices, int ksplit,
-                           int chunk_len, uint64_t timeout_ns, int32_t *err) {
+                           int chunk_len, uint64_t timeout_ns, int32_t *err, int stall) {
     using L = KsTiled<CW>;
     extern __shared__ __align__(128) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kKsThreads, 2)
             bulk_copy_g2s(dst + j * kKsBase * L::rs * 4, blk + j * (kKsBase - 1) * L::rs, L::copy_bytes, bar);
     };
     int issued = 0;  // meaningful in thread 0 only
-    if (tid == 0)
+    if (tid == 0 && !stall)  // stall: failure-detection test hook, no copy is ever issued
         for (; issued < L::stages && issued < i_count; issued++) issue(issued, issued);
 
     uint32_t acc[CW];
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kKsThreads, 2)
             failed = true;
             break;
         }
-        if (tid == 0 && issued < i_count) {
+        if (tid == 0 && !stall && issued < i_count) {
             issue(issued, s);
             issued++;
         }
@@ -279,7 +279,7 @@ template <int C, int G>
 __global__ void __launch_bounds__(256, 1)
     keyswitch_regkey_kernel(const int32_t *__restrict__ rows, const uint32_t *__restrict__ in, int in_stride,
                             uint32_t *__restrict__ out, int count, int n, int kN, int slices, int ksplit,
-                            int chunk_len, uint64_t timeout_ns, int32_t *err) {
+                            int chunk_len, uint64_t timeout_ns, int32_t *err, int stall) {
     using L = KsRegKey<C, G>;
     extern __shared__ __align__(128) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(256, 1)
         bulk_copy_g2s(smem_addr(ring + s * L::stage_words), src + (size_t)q * L::stage_words, L::stage_bytes, bar);
     };
     int issued = 0;  // meaningful in thread 0 only
-    if (tid == 0)
+    if (tid == 0 && !stall)  // stall: failure-detection test hook, no copy is ever issued
         for (; issued < L::stages && issued < i_count; issued++) issue(issued, issued);
 
     uint32_t acc[G][C];
@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(256, 1)
             failed = true;
             break;
         }
-        if (tid == 0 && issued < i_count) {
+        if (tid == 0 && !stall && issued < i_count) {
             issue(issued, st_i);
             issued++;
         }
@@ -445,7 +445,7 @@ cudaError_t launch_tiled(const CloudKey &ck, int count, const int32_t *in, int i
     }
     keyswitch_tiled_kernel<CW><<<units * ksplit, kKsThreads, L::smem_bytes, s>>>(
         ck.dksk.tiles, reinterpret_cast<const uint32_t *>(in), in_stride, reinterpret_cast<uint32_t *>(out), count,
-        p.n, kN, ck.dksk.tile_slices, ksplit, chunk_len, ck.wait_timeout_ns, ck.d_err);
+        p.n, kN, ck.dksk.tile_slices, ksplit, chunk_len, ck.wait_timeout_ns, ck.d_err, ck.stall_producer);
     return cudaGetLastError();
 }
 
@@ -518,7 +518,7 @@ cudaError_t launch_regkey(const CloudKey &ck, int count, const int32_t *in, int 
     }
     keyswitch_regkey_kernel<C, G><<<units * ksplit, 256, L::smem_bytes, s>>>(
         ck.dksk.rk, reinterpret_cast<const uint32_t *>(in), in_stride, reinterpret_cast<uint32_t *>(out), count,
-        p.n, kN, ck.dksk.rk_slices, ksplit, chunk_len, ck.wait_timeout_ns, ck.d_err);
+        p.n, kN, ck.dksk.rk_slices, ksplit, chunk_len, ck.wait_timeout_ns, ck.d_err, ck.stall_producer);
     return cudaGetLastError();
 }
 
