@@ -17,14 +17,15 @@ static int check(const char *name, int got, int want, int *fails) {
 
 int main(int argc, char **argv) {
     int precision = argc > 1 ? atoi(argv[1]) : 0;
+    const int lambda = argc > 2 ? atoi(argv[2]) : 110;  /* <= 80: the reference's 80-bit set */
     uint32_t seed[] = {314, 42, 2024};
     tfhe_random_generator_setSeed(seed, 3);
     tfhe_b200_set_precision(precision);
 
-    TFheGateBootstrappingParameterSet *params = new_default_gate_bootstrapping_parameters(110);
+    TFheGateBootstrappingParameterSet *params = new_default_gate_bootstrapping_parameters(lambda);
     TFheGateBootstrappingSecretKeySet *key = new_random_gate_bootstrapping_secret_keyset(params);
     const TFheGateBootstrappingCloudKeySet *ck = &key->cloud;
-    if (params->in_out_params->n != 630 || params->tgsw_params->tlwe_params->N != 1024) return 2;
+    if (params->in_out_params->n != (lambda <= 80 ? 500 : 630) || params->tgsw_params->tlwe_params->N != 1024) return 2;
 
     enum { NB = 8 };
     LweSample *a = new_gate_bootstrapping_ciphertext_array(NB, params);

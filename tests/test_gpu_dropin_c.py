@@ -1,6 +1,7 @@
 """The drop-in boundary exercised the way a reference user would: a C program written against the
 reference's gate API (tests/c/dropin_gates.c) is compiled with gcc against include/tfhe.h, linked
-with libtfhe_b200.so and run; every gate must decrypt to its truth table, in both precision forms."""
+with libtfhe_b200.so and run; every gate must decrypt to its truth table, in both precision forms and
+for both of the reference's default parameter sets."""
 import os
 import subprocess
 
@@ -21,7 +22,8 @@ def program(tmp_path_factory):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_c_program_against_dropin_header(program, precision):
-    res = subprocess.run([program, str(precision)], capture_output=True, text=True, timeout=600)
+@pytest.mark.parametrize("lam", [110, 80])  # the 128-bit default and the 80-bit set
+def test_c_program_against_dropin_header(program, precision, lam):
+    res = subprocess.run([program, str(precision), str(lam)], capture_output=True, text=True, timeout=600)
     assert res.returncode == 0, res.stdout + res.stderr
     assert res.stdout.strip().endswith("OK")

@@ -219,6 +219,38 @@ def test_all_gates_default_params_truth_tables(default_keys, precision):
         assert (bits == TRUTH[code](a, b, c)).all(), f"gate {tb.api.GATE_NAMES[code]}"
 
 
+@pytest.fixture(scope="module")
+def keys80():
+    p = tb.default_params(80)
+    sk, ck = tb.keygen(p, seed=80)
+    ck.to_device(0)
+    return p, sk, ck
+
+
+@pytest.mark.parametrize("precision", [tb.FP64, tb.SPLIT_FP32])
+def test_80bit_params_all_gates_and_a_4096_batch(keys80, precision):
+    # the reference's 80-bit set (n=500, l=2, Bgbit=10): every gate's truth table, then 4096 NANDs
+    p, sk, ck = keys80
+    assert (p.n, p.l, p.Bgbit) == (500, 2, 10)
+    rng = np.random.default_rng(80 + precision)
+    a, b, c = rng.integers(0, 2, (3, 64))
+    ca, cb, cc = sk.encrypt(a, seed=1), sk.encrypt(b, seed=2), sk.encrypt(c, seed=3)
+    for code in range(13):
+        bits, _ = sk.decrypt(ck.gate(code, ca, cb, cc if code == 10 else None, precision=precision))
+        assert (bits == TRUTH[code](a, b, c)).all(), f"gate {tb.api.GATE_NAMES[code]}"
+    x, y = rng.integers(0, 2, (2, 4096))
+    bits, ph = sk.decrypt(ck.gate(tb.api.NAND, sk.encrypt(x, seed=4), sk.encrypt(y, seed=5), precision=precision))
+    assert (bits == 1 - (x & y)).all()
+    # outputs sit at +-1/8 = +-2^29 Torus32 units; a decryption error needs |noise| > 2^29.  With
+    # 10-bit digits the split form's low limb carries S = 27 bits, so its FP32 error adds to the
+    # noise; both forms keep the rms far below the margin.
+    err = (ph.astype(np.int64) - np.where(bits == 1, 2**29, -2**29) + 2**31) % 2**32 - 2**31
+    rms = float(np.sqrt((err.astype(np.float64) ** 2).mean()))
+    print(f"80-bit set, precision {precision}: output noise rms 2^{np.log2(rms):.2f}, max 2^{np.log2(np.abs(err).max()):.2f}")
+    # measured: FP64 rms 2^24.1 (the reference's precision), split 2^26.0 (the low limb's FP32 error)
+    assert rms < (2**25 if precision == tb.FP64 else 2**26.5)
+
+
 @pytest.mark.parametrize("precision", [tb.FP64, tb.SPLIT_FP32])
 def test_nand_batch_4096_decrypts_and_noise_matches_reference(default_keys, golden_dir, precision):
     # 4096 NANDs in one batch; output noise variance (phase - (+-1/8)) against the reference's

@@ -355,11 +355,11 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
 
 // ---- launch -------------------------------------------------------------------------------------
 
-template <typename T, int N, bool SPLIT, int G, int D>
+template <typename T, int N, int L, bool SPLIT, int G, int D>
 static cudaError_t launch_g(const BrArgs &a, cudaStream_t s) {
     using Lay = BrLayout<T, N, 1, G, D>;
     const size_t smem = Lay::bytes(a.nsteps);
-    auto kern = blind_rotate_kernel<T, N, 1, 3, SPLIT, G, D>;
+    auto kern = blind_rotate_kernel<T, N, 1, L, SPLIT, G, D>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = (a.boots + G - 1) / G;
@@ -368,37 +368,39 @@ static cudaError_t launch_g(const BrArgs &a, cudaStream_t s) {
 }
 
 int blind_rotate_supported(const tfheb_params &p) {
-    if (p.k != 1 || p.l != 3) return 0;
-    return p.N == 512 || p.N == 1024 || p.N == 2048;
+    return br_variants(p.N, p.l, p.k == 1 ? TFHEB_FP64 : -1, nullptr, nullptr, 0) > 0;
 }
 
 // Compiled launch variants: (ring degree, precision, bootstraps per CTA G, key-ring depth D).
 // Every variant's shared memory stays within 227 KB.  The first variant of a (N, precision) pair is
 // the default; tfheb_autotune times all of them on the device and keeps the fastest per key.
 struct BrVariant {
-    int N, precision, G, D;
+    int N, l, precision, G, D;
     cudaError_t (*launch)(const BrArgs &, cudaStream_t);
 };
 static const BrVariant kBrVariants[] = {
-    {1024, TFHEB_SPLIT_FP32, 7, 4, launch_g<float, 1024, true, 7, 4>},
-    {1024, TFHEB_SPLIT_FP32, 5, 4, launch_g<float, 1024, true, 5, 4>},
-    {1024, TFHEB_SPLIT_FP32, 4, 4, launch_g<float, 1024, true, 4, 4>},
-    {1024, TFHEB_FP64, 3, 4, launch_g<double, 1024, false, 3, 4>},
-    {1024, TFHEB_FP64, 4, 4, launch_g<double, 1024, false, 4, 4>},
-    {1024, TFHEB_FP64, 4, 6, launch_g<double, 1024, false, 4, 6>},
-    {1024, TFHEB_FP64, 2, 4, launch_g<double, 1024, false, 2, 4>},
-    {2048, TFHEB_SPLIT_FP32, 3, 3, launch_g<float, 2048, true, 3, 3>},
-    {2048, TFHEB_SPLIT_FP32, 2, 3, launch_g<float, 2048, true, 2, 3>},
-    {2048, TFHEB_FP64, 2, 3, launch_g<double, 2048, false, 2, 3>},
-    {2048, TFHEB_FP64, 1, 4, launch_g<double, 2048, false, 1, 4>},
-    {512, TFHEB_SPLIT_FP32, 8, 4, launch_g<float, 512, true, 8, 4>},
-    {512, TFHEB_FP64, 8, 4, launch_g<double, 512, false, 8, 4>},
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 4, launch_g<float, 1024, 3, true, 7, 4>},
+    {1024, 3, TFHEB_SPLIT_FP32, 5, 4, launch_g<float, 1024, 3, true, 5, 4>},
+    {1024, 3, TFHEB_SPLIT_FP32, 4, 4, launch_g<float, 1024, 3, true, 4, 4>},
+    {1024, 3, TFHEB_FP64, 3, 4, launch_g<double, 1024, 3, false, 3, 4>},
+    {1024, 3, TFHEB_FP64, 4, 4, launch_g<double, 1024, 3, false, 4, 4>},
+    {1024, 3, TFHEB_FP64, 4, 6, launch_g<double, 1024, 3, false, 4, 6>},
+    {1024, 3, TFHEB_FP64, 2, 4, launch_g<double, 1024, 3, false, 2, 4>},
+    {2048, 3, TFHEB_SPLIT_FP32, 3, 3, launch_g<float, 2048, 3, true, 3, 3>},
+    {2048, 3, TFHEB_SPLIT_FP32, 2, 3, launch_g<float, 2048, 3, true, 2, 3>},
+    {2048, 3, TFHEB_FP64, 2, 3, launch_g<double, 2048, 3, false, 2, 3>},
+    {2048, 3, TFHEB_FP64, 1, 4, launch_g<double, 2048, 3, false, 1, 4>},
+    {512, 3, TFHEB_SPLIT_FP32, 8, 4, launch_g<float, 512, 3, true, 8, 4>},
+    {512, 3, TFHEB_FP64, 8, 4, launch_g<double, 512, 3, false, 8, 4>},
+    // the 80-bit parameter set (n = 500, l = 2, Bgbit = 10; tfhe_gate_bootstrapping.cpp:23-48)
+    {1024, 2, TFHEB_SPLIT_FP32, 7, 4, launch_g<float, 1024, 2, true, 7, 4>},
+    {1024, 2, TFHEB_FP64, 4, 4, launch_g<double, 1024, 2, false, 4, 4>},
 };
 
-int br_variants(int N, int precision, int *G, int *D, int cap) {
+int br_variants(int N, int l, int precision, int *G, int *D, int cap) {
     int n = 0;
     for (const auto &v : kBrVariants)
-        if (v.N == N && v.precision == precision) {
+        if (v.N == N && v.l == l && v.precision == precision) {
             if (n < cap) {
                 if (G) G[n] = v.G;
                 if (D) D[n] = v.D;
@@ -417,7 +419,7 @@ cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const Devi
              nsteps, mu, p.Bgbit, bsk.split_shift, d_err, timeout_ns, stall_producer};
     int seen = 0;
     for (const auto &v : kBrVariants)
-        if (v.N == p.N && v.precision == precision) {
+        if (v.N == p.N && v.l == p.l && v.precision == precision) {
             if (seen == variant) return v.launch(a, s);
             seen++;
         }

@@ -614,13 +614,14 @@ tfheb_status tfheb_set_wait_timeout(tfheb_cloud_key *c, uint64_t timeout_ns) {
 tfheb_status tfheb_br_variants(int32_t N, int32_t precision, int32_t *teams_per_cta, int32_t *ring_depth,
                                int32_t cap, int32_t *count) {
     if (!count) return TFHEB_ERR_INVALID;
-    *count = br_variants(N, precision, teams_per_cta, ring_depth, cap);
+    *count = br_variants(N, 3, precision, teams_per_cta, ring_depth, cap);
     return TFHEB_OK;
 }
 
 tfheb_status tfheb_set_br_variant(tfheb_cloud_key *c, int32_t precision, int32_t variant) {
     if (!c || (precision != TFHEB_FP64 && precision != TFHEB_SPLIT_FP32)) return TFHEB_ERR_INVALID;
-    if (variant < 0 || variant >= br_variants(c->ck.p.N, precision, nullptr, nullptr, 0)) return TFHEB_ERR_INVALID;
+    if (variant < 0 || variant >= br_variants(c->ck.p.N, c->ck.p.l, precision, nullptr, nullptr, 0))
+        return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
     c->ck.br_variant[precision] = variant;
     return TFHEB_OK;
@@ -657,7 +658,7 @@ tfheb_status tfheb_autotune(tfheb_cloud_key *c, int32_t precision, int32_t boots
         v = (int32_t)(x % (uint64_t)(2 * p.N));
     }
     TFHEB_CUDA(cudaMemcpy(ck.d_bara, bara.data(), bara.size() * 4, cudaMemcpyHostToDevice));
-    const int nv = br_variants(p.N, precision, nullptr, nullptr, 0);
+    const int nv = br_variants(p.N, p.l, precision, nullptr, nullptr, 0);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);

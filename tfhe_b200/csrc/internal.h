@@ -137,8 +137,8 @@ cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const Devi
                                 int bara_stride, int boots, int nsteps, int32_t mu, const int32_t *acc_in,
                                 int32_t *acc_out, cudaStream_t s, int32_t *d_err, int stall_producer,
                                 uint64_t timeout_ns, int variant);
-// Launch variants compiled for (N, precision): count, and their (G, D) into the arrays (up to cap).
-int br_variants(int N, int precision, int *G, int *D, int cap);
+// Launch variants compiled for (N, l, precision): count, and their (G, D) into the arrays (up to cap).
+int br_variants(int N, int l, int precision, int *G, int *D, int cap);
 cudaError_t launch_extract(const tfheb_params &p, const GateDesc *d_desc, int count, const int32_t *acc,
                            int32_t *out, int out_stride, cudaStream_t s);
 // keyswitch.cu: device key upload (both layouts) and the keyswitch of `count` extracted samples

@@ -175,7 +175,7 @@ cudaError_t enqueue_netlist(tfheb_netlist *nl, CloudKey &ck, int precision, int3
 int wave_bootstraps(const CloudKey &ck, int precision) {
     int sms = 0, G[16] = {0}, D[16] = {0};
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ck.device);
-    const int nv = br_variants(ck.p.N, precision, G, D, 16);
+    const int nv = br_variants(ck.p.N, ck.p.l, precision, G, D, 16);
     const int v = ck.br_variant[precision];
     return std::max(1, sms) * (nv > 0 && v < nv ? G[v] : 1);
 }
