@@ -214,18 +214,22 @@ __host__ __device__ constexpr double fold_sin(int n) { return n == 0 ? 0.0 : fol
 //           pattern (each of a thread's eight addresses is a per-stage base plus a compile-time
 //           offset) and, simulated over all stores and loads of the 8*8*8 and 8*8*8*2 plans,
 //           bank-conflict free for 16-byte accesses;
-//   float:  separate re / im arrays of 32-bit words, XOR-swizzled p ^ ((p >> 3) & 31), which is
-//           conflict free for 32-bit accesses (interleaved float2 with any affine padding leaves
-//           2-way conflicts on the stride-8 stage: measured ~9x more conflicts on B200).
+//   float:  interleaved float2, XOR-swizzled p ^ ((p >> 2) & 7) ^ ((p >> 3) & 31).  An 8-byte
+//           warp access is served as two half-warp wavefronts; for every store and load of the
+//           8*8*4, 8*8*8 and 8*8*8*2 plans this map puts a half-warp's sixteen float2 on sixteen
+//           distinct bank pairs, so each access takes the minimum two wavefronts (measured on B200
+//           for the 8*8*8 plan: 2.00 per instruction, no conflicts; affine padding p + (p >> 3)
+//           measured 2.50, the bare index 6.50).  Half the instructions of two 32-bit arrays.
 template <typename T, int M>
 struct Exch;
 template <int M>
 struct Exch<double, M> {
-    static constexpr int bytes = 16 * (M + (M >> 3));
+    static constexpr int slots = M + (M >> 3);
+    static constexpr int bytes = 16 * slots;
     // element index of position p; every stage pattern is affine in it: idx(base + d) = idx(base) + delta
     __host__ __device__ static constexpr int index(int p) { return p + (p >> 3); }
     __host__ __device__ static constexpr int delta(int p, int p0) { return index(p) - index(p0); }
-    __device__ static __forceinline__ int combine(int base, int d) { return base + d; }
+    __host__ __device__ static constexpr int combine(int base, int d) { return base + d; }
     __device__ static __forceinline__ void put(void *buf, int i, cplx<double> v) {
         reinterpret_cast<cplx<double> *>(buf)[i] = v;
     }
@@ -235,20 +239,19 @@ struct Exch<double, M> {
 };
 template <int M>
 struct Exch<float, M> {
-    static constexpr int bytes = 8 * M;
+    static constexpr int slots = M;
+    static constexpr int bytes = 8 * slots;
     // XOR swizzle; every stage pattern is XOR-separable: idx(pos(t,c,n2)) = idx(pos(t,0,0)) ^ delta(c,n2)
-    // (checked for the 8*8*4, 8*8*8 and 8*8*8*2 plans), so each access costs one XOR with a constant
-    __host__ __device__ static constexpr int index(int p) { return p ^ ((p >> 3) & 31); }
+    // (TeamFft asserts it at compile time), so each access costs one XOR with a constant
+    __host__ __device__ static constexpr int index(int p) { return p ^ ((p >> 2) & 7) ^ ((p >> 3) & 31); }
     __host__ __device__ static constexpr int delta(int p, int p0) { return index(p) ^ index(p0); }
-    __device__ static __forceinline__ int combine(int base, int d) { return base ^ d; }
+    __host__ __device__ static constexpr int combine(int base, int d) { return base ^ d; }
     __device__ static __forceinline__ void put(void *buf, int i, cplx<float> v) {
-        float *re = reinterpret_cast<float *>(buf);
-        re[i] = v.re;
-        re[M + i] = v.im;
+        reinterpret_cast<float2 *>(buf)[i] = make_float2(v.re, v.im);
     }
     __device__ static __forceinline__ cplx<float> get(const void *buf, int i) {
-        const float *re = reinterpret_cast<const float *>(buf);
-        return {re[i], re[M + i]};
+        const float2 v = reinterpret_cast<const float2 *>(buf)[i];
+        return {v.x, v.y};
     }
 };
 
@@ -294,8 +297,33 @@ struct TeamFft {
         return Exch<T, M>::delta(pos<S>(0, c, n2), pos<S>(0, 0, 0));
     }
 
+    // The exchange layout must be a one-to-one map of the M positions into the buffer, and on every
+    // stage each register's index must be the thread's base index combined with a constant.
+    static constexpr bool exchange_layout_valid() {
+        using X = Exch<T, M>;
+        bool seen[X::slots] = {};
+        for (int p = 0; p < M; p++) {
+            const int i = X::index(p);
+            if (i < 0 || i >= X::slots || seen[i]) return false;
+            seen[i] = true;
+        }
+        for (int S = 0; S < NS; S++) {
+            const int L = stage_len<M>(S), r = FftPlan<M>::radix(S), st = L / r;
+            for (int t = 0; t < NT; t++)
+                for (int c = 0; c < R / r; c++)
+                    for (int n2 = 0; n2 < r; n2++) {
+                        const int b0 = NT * c, b = t + NT * c;
+                        const int p0 = (b0 / st) * L + b0 % st + st * n2, p = (b / st) * L + b % st + st * n2;
+                        const int t0 = (t / st) * L + t % st;
+                        if (X::combine(X::index(t0), X::delta(p0, 0)) != X::index(p)) return false;
+                    }
+        }
+        return true;
+    }
+
     template <int S>
     __device__ static __forceinline__ void store(const cplx<T> *x, void *buf, int t) {
+        static_assert(exchange_layout_valid(), "exchange layout not one-to-one or not separable on some stage");
         constexpr int r = Stage<M, S>::r;
         const int base = Exch<T, M>::index(pos<S>(t, 0, 0));
 #pragma unroll
