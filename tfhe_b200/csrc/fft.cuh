@@ -209,27 +209,57 @@ __host__ __device__ constexpr double fold_cos(int n) {
 }
 __host__ __device__ constexpr double fold_sin(int n) { return n == 0 ? 0.0 : fold_cos(8 - n); }
 
-// Exchange buffer of one team FFT (M complex points), laid out per precision:
-//   double: interleaved double2 with one pad element every 8 -- affine on every stage's access
-//           pattern (each of a thread's eight addresses is a per-stage base plus a compile-time
-//           offset) and, simulated over all stores and loads of the 8*8*8 and 8*8*8*2 plans,
-//           bank-conflict free for 16-byte accesses;
-//   float:  interleaved float2, XOR-swizzled p ^ ((p >> 2) & 7) ^ ((p >> 3) & 31).  An 8-byte
-//           warp access is served as two half-warp wavefronts; for every store and load of the
-//           8*8*4, 8*8*8 and 8*8*8*2 plans this map puts a half-warp's sixteen float2 on sixteen
-//           distinct bank pairs, so each access takes the minimum two wavefronts (measured on B200
-//           for the 8*8*8 plan: 2.00 per instruction, no conflicts; affine padding p + (p >> 3)
-//           measured 2.50, the bare index 6.50).  Half the instructions of two 32-bit arrays.
+// Exchange buffers of one team FFT (M complex points).  Exchange E moves the points from stage E's
+// registers to stage E+1's (the inverse runs the same exchanges backwards); its layout maps point p
+// to an element index.  Every layout is separable on both of its stages: the index of a thread's
+// register (c, n2) is the thread's base index combined with a compile-time constant, by addition
+// (the constant folds into the load/store offset) or, for the XOR swizzle, by one XOR per access.
+// TeamFft asserts both properties at compile time.
+//   double: interleaved double2 with one pad element every 8, p + (p >> 3), for every exchange;
+//           simulated over all stores and loads of the 8*8*8 and 8*8*8*2 plans, conflict free for
+//           16-byte accesses.
+//   float:  interleaved float2, one map per exchange.  An 8-byte warp access is served as two
+//           half-warp wavefronts, each costing the largest number of distinct 8-byte words on one of
+//           the 16 bank pairs; this model matched the wavefronts measured on B200 for 12 candidate
+//           maps of the 8*8*8 plan.  The maps below reach the minimum of two wavefronts per access on
+//           both stages of their exchange, padded (additive) where such a padding exists and
+//           XOR-swizzled p ^ ((p >> 2) & 7) ^ ((p >> 3) & 31) on the last exchange of the 8*8*8*2
+//           plan, where none does.  A single map for all exchanges (the swizzle) costs a XOR per
+//           access; p + (p >> 3) for all of them costs 2.5 wavefronts per access.
+struct ExchMap {
+    int s1, a, s2, b;  // index = p + a * (p >> s1) + b * (p >> s2)
+    bool swizzle;      // index = p ^ ((p >> 2) & 7) ^ ((p >> 3) & 31) instead
+};
+template <int M>
+__host__ __device__ constexpr ExchMap exch_f32_map(int E) {
+    return M == 256    ? (E == 0 ? ExchMap{5, 4, 6, 0, false} : ExchMap{2, 1, 6, 4, false})
+           : M == 512  ? (E == 0 ? ExchMap{5, 4, 6, 0, false} : ExchMap{3, 1, 4, 0, false})
+           : M == 1024 ? (E == 0   ? ExchMap{2, 0, 3, 0, false}
+                          : E == 1 ? ExchMap{4, 2, 5, 0, false}
+                                   : ExchMap{0, 0, 0, 0, true})
+                       : ExchMap{2, 0, 3, 0, false};
+}
+template <int M>
+__host__ __device__ constexpr int exch_f32_index(int E, int p) {
+    const ExchMap m = exch_f32_map<M>(E);
+    return m.swizzle ? p ^ ((p >> 2) & 7) ^ ((p >> 3) & 31) : p + m.a * (p >> m.s1) + m.b * (p >> m.s2);
+}
+template <int M>
+__host__ __device__ constexpr int exch_f32_slots() {
+    int n = 0;
+    for (int E = 0; E + 1 < FftPlan<M>::NS; E++)
+        for (int p = 0; p < M; p++) n = n > exch_f32_index<M>(E, p) + 1 ? n : exch_f32_index<M>(E, p) + 1;
+    return n;
+}
+
 template <typename T, int M>
 struct Exch;
 template <int M>
 struct Exch<double, M> {
     static constexpr int slots = M + (M >> 3);
     static constexpr int bytes = 16 * slots;
-    // element index of position p; every stage pattern is affine in it: idx(base + d) = idx(base) + delta
-    __host__ __device__ static constexpr int index(int p) { return p + (p >> 3); }
-    __host__ __device__ static constexpr int delta(int p, int p0) { return index(p) - index(p0); }
-    __host__ __device__ static constexpr int combine(int base, int d) { return base + d; }
+    __host__ __device__ static constexpr bool additive(int) { return true; }
+    __host__ __device__ static constexpr int index(int, int p) { return p + (p >> 3); }
     __device__ static __forceinline__ void put(void *buf, int i, cplx<double> v) {
         reinterpret_cast<cplx<double> *>(buf)[i] = v;
     }
@@ -239,13 +269,10 @@ struct Exch<double, M> {
 };
 template <int M>
 struct Exch<float, M> {
-    static constexpr int slots = M;
+    static constexpr int slots = exch_f32_slots<M>();
     static constexpr int bytes = 8 * slots;
-    // XOR swizzle; every stage pattern is XOR-separable: idx(pos(t,c,n2)) = idx(pos(t,0,0)) ^ delta(c,n2)
-    // (TeamFft asserts it at compile time), so each access costs one XOR with a constant
-    __host__ __device__ static constexpr int index(int p) { return p ^ ((p >> 2) & 7) ^ ((p >> 3) & 31); }
-    __host__ __device__ static constexpr int delta(int p, int p0) { return index(p) ^ index(p0); }
-    __host__ __device__ static constexpr int combine(int base, int d) { return base ^ d; }
+    __host__ __device__ static constexpr bool additive(int E) { return !exch_f32_map<M>(E).swizzle; }
+    __host__ __device__ static constexpr int index(int E, int p) { return exch_f32_index<M>(E, p); }
     __device__ static __forceinline__ void put(void *buf, int i, cplx<float> v) {
         reinterpret_cast<float2 *>(buf)[i] = make_float2(v.re, v.im);
     }
@@ -291,57 +318,68 @@ struct TeamFft {
         const int q = b / st, n1 = b - q * st;
         return q * L + n1 + st * n2;
     }
-    // compile-time part of the exchange index of register (c, n2) at stage S
-    template <int S>
+    // index of point p in exchange E's buffer; base index combined with a compile-time constant
+    __host__ __device__ static constexpr int xindex(int E, int p) { return Exch<T, M>::index(E, p); }
+    __host__ __device__ static constexpr int xcombine(int E, int base, int d) {
+        return Exch<T, M>::additive(E) ? base + d : base ^ d;
+    }
+    // compile-time part of the index of register (c, n2) at stage S in exchange E (pos<S>(0,0,0) = 0)
+    template <int S, int E>
     __host__ __device__ static constexpr int delta(int c, int n2) {
-        return Exch<T, M>::delta(pos<S>(0, c, n2), pos<S>(0, 0, 0));
+        return Exch<T, M>::additive(E) ? xindex(E, pos<S>(0, c, n2)) - xindex(E, 0)
+                                       : xindex(E, pos<S>(0, c, n2)) ^ xindex(E, 0);
     }
 
-    // The exchange layout must be a one-to-one map of the M positions into the buffer, and on every
-    // stage each register's index must be the thread's base index combined with a constant.
+    // Every exchange layout must be a one-to-one map of the M positions into the buffer, and on both
+    // of its stages each register's index must be the thread's base index combined with a constant.
     static constexpr bool exchange_layout_valid() {
         using X = Exch<T, M>;
-        bool seen[X::slots] = {};
-        for (int p = 0; p < M; p++) {
-            const int i = X::index(p);
-            if (i < 0 || i >= X::slots || seen[i]) return false;
-            seen[i] = true;
-        }
-        for (int S = 0; S < NS; S++) {
-            const int L = stage_len<M>(S), r = FftPlan<M>::radix(S), st = L / r;
-            for (int t = 0; t < NT; t++)
-                for (int c = 0; c < R / r; c++)
-                    for (int n2 = 0; n2 < r; n2++) {
-                        const int b0 = NT * c, b = t + NT * c;
-                        const int p0 = (b0 / st) * L + b0 % st + st * n2, p = (b / st) * L + b % st + st * n2;
-                        const int t0 = (t / st) * L + t % st;
-                        if (X::combine(X::index(t0), X::delta(p0, 0)) != X::index(p)) return false;
-                    }
+        for (int E = 0; E + 1 < NS; E++) {
+            bool seen[X::slots] = {};
+            for (int p = 0; p < M; p++) {
+                const int i = xindex(E, p);
+                if (i < 0 || i >= X::slots || seen[i]) return false;
+                seen[i] = true;
+            }
+            for (int S = E; S <= E + 1; S++) {
+                const int L = stage_len<M>(S), r = FftPlan<M>::radix(S), st = L / r;
+                for (int t = 0; t < NT; t++)
+                    for (int c = 0; c < R / r; c++)
+                        for (int n2 = 0; n2 < r; n2++) {
+                            const int b0 = NT * c, b = t + NT * c;
+                            const int p0 = (b0 / st) * L + b0 % st + st * n2;
+                            const int p = (b / st) * L + b % st + st * n2;
+                            const int t0 = (t / st) * L + t % st;
+                            const int d = X::additive(E) ? xindex(E, p0) - xindex(E, 0) : xindex(E, p0) ^ xindex(E, 0);
+                            if (xcombine(E, xindex(E, t0), d) != xindex(E, p)) return false;
+                        }
+            }
         }
         return true;
     }
 
-    template <int S>
+    // stage S's registers to / from exchange E's buffer
+    template <int S, int E>
     __device__ static __forceinline__ void store(const cplx<T> *x, void *buf, int t) {
         static_assert(exchange_layout_valid(), "exchange layout not one-to-one or not separable on some stage");
         constexpr int r = Stage<M, S>::r;
-        const int base = Exch<T, M>::index(pos<S>(t, 0, 0));
+        const int base = xindex(E, pos<S>(t, 0, 0));
 #pragma unroll
         for (int c = 0; c < R / r; c++)
 #pragma unroll
             for (int n2 = 0; n2 < r; n2++)
-                Exch<T, M>::put(buf, Exch<T, M>::combine(base, delta<S>(c, n2)), x[c * r + n2]);
+                Exch<T, M>::put(buf, xcombine(E, base, delta<S, E>(c, n2)), x[c * r + n2]);
     }
 
-    template <int S>
+    template <int S, int E>
     __device__ static __forceinline__ void load(cplx<T> *x, const void *buf, int t) {
         constexpr int r = Stage<M, S>::r;
-        const int base = Exch<T, M>::index(pos<S>(t, 0, 0));
+        const int base = xindex(E, pos<S>(t, 0, 0));
 #pragma unroll
         for (int c = 0; c < R / r; c++)
 #pragma unroll
             for (int n2 = 0; n2 < r; n2++)
-                x[c * r + n2] = Exch<T, M>::get(buf, Exch<T, M>::combine(base, delta<S>(c, n2)));
+                x[c * r + n2] = Exch<T, M>::get(buf, xcombine(E, base, delta<S, E>(c, n2)));
     }
 
     template <int S, bool INV>
@@ -386,9 +424,9 @@ struct TeamFft {
         twiddle<S, false>(x, tw, t);
         if constexpr (S + 1 < NS) {
             void *buf = xp.next();
-            store<S>(x, buf, t);
+            store<S, S>(x, buf, t);
             team_sync(bar_id, NT);
-            load<S + 1>(x, buf, t);
+            load<S + 1, S>(x, buf, t);
             if (xp.stride == 0) team_sync(bar_id, NT);
             forward_from<S + 1>(x, xp, tw, t, bar_id);
         }
@@ -402,9 +440,9 @@ struct TeamFft {
         for (int c = 0; c < R / r; c++) dft<T, true, r>(x + c * r);
         if constexpr (S > 0) {
             void *buf = xp.next();
-            store<S>(x, buf, t);
+            store<S, S - 1>(x, buf, t);
             team_sync(bar_id, NT);
-            load<S - 1>(x, buf, t);
+            load<S - 1, S - 1>(x, buf, t);
             if (xp.stride == 0) team_sync(bar_id, NT);
             inverse_from<S - 1>(x, xp, tw, t, bar_id);
         }
