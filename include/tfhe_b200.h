@@ -170,13 +170,18 @@ tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *ck, int32_t gate, int32_t 
                                      const int32_t *d_a, const int32_t *d_b, const int32_t *d_c, int32_t *d_out,
                                      void *stream);
 
-/* Mixed gate types (gates[count] codes) on device buffers: input i of gate g is row idx_i[g] of the
- * wire array d_wires ([*][n+1]); outputs go to rows out_idx[g] of d_wires.  Index arrays are host
- * arrays; they are uploaded once and cached per call site by the netlist API below. */
+/* Mixed gate types in one batch on a device wire array (no reference counterpart; the reference
+ * calls the gate functions of boot-gates.cpp one at a time).  d_wires holds num_wires rows of n+1
+ * int32.  Gate g (code gates[g]) reads rows idx_a[g], idx_b[g] (binary gates and MUX) and idx_c[g]
+ * (MUX) and writes row out_idx[g]; NOT/COPY read idx_a only.  Every operand is read before any
+ * output is written, so an output may overwrite an operand of the same batch.  The index arrays are
+ * host arrays, checked on the host (rows in range, no output row twice) and uploaded on each call;
+ * scratch is stream-ordered (cudaMallocAsync / cudaFreeAsync).  Asynchronous on `stream` (NULL: the
+ * key's stream). */
 tfheb_status tfheb_gate_batch_mixed_device(tfheb_cloud_key *ck, int32_t precision, int32_t count,
                                            const int32_t *gates, const int32_t *idx_a, const int32_t *idx_b,
                                            const int32_t *idx_c, const int32_t *out_idx, int32_t *d_wires,
-                                           void *stream);
+                                           int32_t num_wires, void *stream);
 
 /* Hot-path pieces on device buffers (the scalar reference functions, batched):
  *   tfheb_bootstrap_woks_device  -> tfhe_bootstrap_woKS_FFT (lwe-bootstrapping-functions-fft.cpp:169-200)
@@ -260,6 +265,24 @@ tfheb_status tfheb_netlist_info(const tfheb_netlist *nl, int32_t *num_levels, in
 tfheb_status tfheb_netlist_run(tfheb_netlist *nl, int32_t precision, int32_t *d_wires, int32_t use_graph,
                                void *stream);
 void tfheb_netlist_free(tfheb_netlist *nl);
+
+/* The same netlist sharded across several cloud keys, each on its own GPU (replica sharding of
+ * netlist levels; no reference counterpart).  The keys must be distinct, share one parameter set
+ * and be on their devices (two keys may share a device).  create: one level assignment for all keys,
+ * packed for their waves together; every level's bootstrapped gates are cut into one contiguous run
+ * per key with balanced bootstrap counts (a MUX counts two); NOT/COPY gates run on every key.  Each key
+ * holds a full wire array.  run: wires is a HOST array [num_inputs+num_gates][n+1] whose input rows the
+ * caller filled; they are copied to every key.  Per level, every key evaluates its run on its own
+ * stream, then copies those output rows into every other key's wire array (peer copies; the next
+ * level waits on them with events, no host synchronisation between levels).  Returns when gate g's
+ * output is in row num_inputs+g of `wires`, bit-identical to tfheb_netlist_run on one key.  Launches
+ * are eager (no CUDA graph). */
+typedef struct tfheb_netlist_multi tfheb_netlist_multi;
+tfheb_status tfheb_netlist_multi_create(tfheb_cloud_key *const *cks, int32_t nkeys, int32_t num_inputs,
+                                        int32_t num_gates, const int32_t *gates, const int32_t *in_a,
+                                        const int32_t *in_b, const int32_t *in_c, tfheb_netlist_multi **out);
+tfheb_status tfheb_netlist_multi_run(tfheb_netlist_multi *nl, int32_t precision, int32_t *wires);
+void tfheb_netlist_multi_free(tfheb_netlist_multi *nl);
 
 /* Allocation-free variant of tfheb_gate_batch_device, for callers that cannot call cudaMalloc
  * (while a CUDA graph is being captured, in real-time or signal-handling code that must not enter

@@ -229,6 +229,17 @@ class CloudKey:
         _check(lib().tfheb_gate_batch_device(self.h, gate, precision, count, _p(d_a), _p(d_b), _p(d_c), _p(d_out),
                                              stream), "tfheb_gate_batch_device")
 
+    def gate_mixed_device(self, gates, idx_a, idx_b, idx_c, out_idx, d_wires, num_wires, precision=FP64,
+                          stream=None):
+        """Mixed gate types over rows of a device wire array (tfheb_gate_batch_mixed_device); the index
+        arrays are host arrays."""
+        L = lib()
+        L.tfheb_gate_batch_mixed_device.argtypes = [_V, _I32, _I32, _V, _V, _V, _V, _V, _V, _I32, _V]
+        g = _i32(gates)
+        ia, ib, ic, io = (_i32(x if x is not None else np.zeros(len(g))) for x in (idx_a, idx_b, idx_c, out_idx))
+        _check(L.tfheb_gate_batch_mixed_device(self.h, precision, len(g), _p(g), _p(ia), _p(ib), _p(ic), _p(io),
+                                               _p(d_wires), num_wires, stream), "tfheb_gate_batch_mixed_device")
+
     def bootstrap_woks_device(self, d_in, d_out, count, mu, precision=FP64, stream=None):
         _check(lib().tfheb_bootstrap_woks_device(self.h, precision, mu, count, _p(d_in), _p(d_out), stream),
                "tfheb_bootstrap_woks_device")
@@ -385,6 +396,50 @@ class Netlist:
     def free(self):
         if self.h:
             lib().tfheb_netlist_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class NetlistMulti:
+    """A netlist sharded across several cloud keys / GPUs (tfheb_netlist_multi_*), evaluated from and
+    to a host wire array."""
+
+    def __init__(self, cks, num_inputs, gates, in_a, in_b=None, in_c=None):
+        L = lib()
+        L.tfheb_netlist_multi_create.argtypes = [_V, _I32, _I32, _I32, _V, _V, _V, _V, ctypes.POINTER(_V)]
+        L.tfheb_netlist_multi_run.argtypes = [_V, _I32, _V]
+        L.tfheb_netlist_multi_free.argtypes = [_V]
+        self.cks = list(cks)
+        self.num_inputs = int(num_inputs)
+        self.gates = _i32(gates)
+        g = len(self.gates)
+        self._a = _i32(in_a)
+        self._b = _i32(in_b if in_b is not None else np.zeros(g))
+        self._c = _i32(in_c if in_c is not None else np.zeros(g))
+        arr = (_V * len(self.cks))(*[k.h for k in self.cks])
+        h = _V()
+        self.h = None
+        _check(L.tfheb_netlist_multi_create(ctypes.cast(arr, _V), len(self.cks), self.num_inputs, g, _p(self.gates),
+                                            _p(self._a), _p(self._b), _p(self._c), ctypes.byref(h)),
+               "tfheb_netlist_multi_create")
+        self.h = h
+
+    def run(self, inputs, precision=FP64):
+        """inputs: [num_inputs][n+1] ciphertexts; returns the wire array [num_inputs+num_gates][n+1]."""
+        inputs = _i32(inputs)
+        wires = np.zeros((self.num_inputs + len(self.gates), inputs.shape[1]), np.int32)
+        wires[:self.num_inputs] = inputs
+        _check(lib().tfheb_netlist_multi_run(self.h, precision, _p(wires)), "tfheb_netlist_multi_run")
+        return wires
+
+    def free(self):
+        if self.h:
+            lib().tfheb_netlist_multi_free(self.h)
             self.h = None
 
     def __del__(self):

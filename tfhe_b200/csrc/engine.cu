@@ -178,7 +178,7 @@ static tfheb_status run_pipeline(CloudKey &ck, int precision, int count, int boo
 }
 
 // Reads and clears the key's device error word (after the stream has been synchronised).
-static tfheb_status check_device_error(CloudKey &ck) {
+tfheb_status check_device_error(CloudKey &ck) {
     int32_t err = 0;
     TFHEB_CUDA(cudaMemcpy(&err, ck.d_err, sizeof(err), cudaMemcpyDeviceToHost));
     if (err) {
@@ -501,15 +501,6 @@ tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precisio
     TFHEB_CUDA(cudaMemcpyAsync(out, dio + 3 * sz, sz * 4, cudaMemcpyDeviceToHost, ck.stream));
     TFHEB_CUDA(cudaStreamSynchronize(ck.stream));
     return check_device_error(ck);
-}
-
-tfheb_status tfheb_gate_batch_mixed_device(tfheb_cloud_key *c, int32_t precision, int32_t count, const int32_t *gates,
-                                           const int32_t *idx_a, const int32_t *idx_b, const int32_t *idx_c,
-                                           const int32_t *out_idx, int32_t *d_wires, void *stream) {
-    (void)c; (void)precision; (void)count; (void)gates; (void)idx_a; (void)idx_b; (void)idx_c; (void)out_idx;
-    (void)d_wires; (void)stream;
-    set_error("mixed batches are evaluated through the netlist API");
-    return TFHEB_ERR_UNSUPPORTED;
 }
 
 tfheb_status tfheb_bootstrap_woks_device(tfheb_cloud_key *c, int32_t precision, int32_t mu, int32_t count,

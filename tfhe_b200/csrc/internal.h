@@ -160,6 +160,9 @@ tfheb_status prepare_device(CloudKey &ck, int precision);
 // Linear combination of a binary gate (boot-gates.cpp:34-319): constant and operand weights.
 void gate_form(int gate, int32_t *cst, int32_t *sa, int32_t *sb);
 int bara_stride_for(const tfheb_params &p);
+// Reads and clears the key's device error word (after the work has finished): TFHEB_ERR_TIMEOUT when
+// a bounded device-side wait expired.
+tfheb_status check_device_error(CloudKey &ck);
 extern std::atomic<int64_t> g_kernel_launches;
 
 // ---- reference file format (io.cu) ----------------------------------------------------------
