@@ -73,12 +73,11 @@ struct DigitConv<double> {
 template <typename T, int N, int K, int G, int D>
 struct BrLayout {
     static constexpr int M = N / 2, NT = M / kR, KP1 = K + 1;
-    static constexpr int TW = tw_offset<M>(FftPlan<M>::NS);
     static constexpr uint32_t chunk = (uint32_t)KP1 * M * 16;  // one key row (step, p): all v, all slots
     static constexpr size_t bars = 0;                           // full[D], empty[D], abort flag
     static constexpr size_t ring = 128;
     static constexpr size_t tables = ring + (size_t)D * chunk;
-    static constexpr size_t tables_bytes = ((sizeof(cplx<T>) * TW) + 15) / 16 * 16;
+    static constexpr size_t tables_bytes = tw_table_bytes<T, M>();
     static constexpr size_t teams = tables + tables_bytes;
     static constexpr size_t team_acc = 4 * (size_t)KP1 * N;
     static constexpr size_t team_xbuf = ((size_t)Exch<T, M>::bytes + 15) / 16 * 16;  // one exchange buffer

@@ -411,7 +411,8 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32
             TFHEB_CUDA(cudaMalloc(&d.tables, tab.size() * sizeof(double)));
             TFHEB_CUDA(cudaMemcpy(d.tables, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
         } else {
-            std::vector<float> tf(tab.begin(), tab.end());
+            std::vector<float> tf;
+            build_tables_f32(p.N, tf);
             TFHEB_CUDA(cudaMalloc(&d.tables, tf.size() * sizeof(float)));
             TFHEB_CUDA(cudaMemcpy(d.tables, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice));
         }

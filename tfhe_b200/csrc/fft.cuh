@@ -201,6 +201,22 @@ __host__ __device__ constexpr int tw_offset(int S) {
     return off;
 }
 
+// FP32 twiddle table, in float4 pairs so that one 16-byte load feeds two registers.  Stage S (radix r,
+// stride st = L/r) holds r/2 float4 per n1 < st at [p][st]: stage 0 pairs {w(2p), w(2p+1)} of the
+// factors above (k2 = 2p, 2p+1; st = NT), stages S >= 1 pairs {w(2p+1), w(2p+2)} (k2 = 2p+1, 2p+2; an
+// odd count ends with a zero pad).  Offsets in float4 units.
+template <int M>
+__host__ __device__ constexpr int tw4_offset(int S) {
+    int off = 0;
+    for (int s = 0; s < S; s++) off += (FftPlan<M>::radix(s) / 2) * (stage_len<M>(s) / FftPlan<M>::radix(s));
+    return off;
+}
+// bytes of the twiddle table of a T transform (a multiple of 16)
+template <typename T, int M>
+__host__ __device__ constexpr int tw_table_bytes() {
+    return sizeof(T) == 4 ? 16 * tw4_offset<M>(FftPlan<M>::NS) : 16 * tw_offset<M>(FftPlan<M>::NS);
+}
+
 // exp(-i pi n / 16), n = 0..7: the per-register part of the twist (NT / N = 1/16 for R = 8)
 __host__ __device__ constexpr double fold_cos(int n) {
     return n == 0 ? 1.0 : n == 1 ? 0.98078528040323044913 : n == 2 ? 0.92387953251128675613
@@ -385,7 +401,32 @@ struct TeamFft {
     template <int S, bool INV>
     __device__ static __forceinline__ void twiddle(cplx<T> *x, const cplx<T> *tw, int t) {
         constexpr int r = Stage<M, S>::r, st = Stage<M, S>::stride;
-        if constexpr (S == 0) {
+        if constexpr (sizeof(T) == 4) {  // paired float4 table (tw4_offset)
+            const float4 *tw4 = reinterpret_cast<const float4 *>(tw) + tw4_offset<M>(S);
+            auto apply = [&](cplx<T> &v, float re, float im) {
+                const cplx<T> w{re, im};
+                v = INV ? cmulconj(v, w) : cmul(v, w);
+            };
+            if constexpr (S == 0) {
+#pragma unroll
+                for (int q = 0; q < r / 2; q++) {
+                    const float4 w = tw4[q * NT + t];
+                    apply(x[2 * q], w.x, w.y);
+                    apply(x[2 * q + 1], w.z, w.w);
+                }
+            } else if constexpr (st > 1) {
+#pragma unroll
+                for (int c = 0; c < R / r; c++) {
+                    const int n1 = (t + NT * c) % st;
+#pragma unroll
+                    for (int q = 0; q < r / 2; q++) {
+                        const float4 w = tw4[q * st + n1];
+                        apply(x[c * r + 2 * q + 1], w.x, w.y);
+                        if (2 * q + 2 < r) apply(x[c * r + 2 * q + 2], w.z, w.w);
+                    }
+                }
+            }
+        } else if constexpr (S == 0) {
 #pragma unroll
             for (int k2 = 0; k2 < r; k2++) {
                 const cplx<T> w = tw[k2 * NT + t];

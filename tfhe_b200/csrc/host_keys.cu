@@ -260,6 +260,31 @@ void tables_m(std::vector<double> &tab) {
     }
 }
 
+// The FP32 table in float4 pairs (tw4_offset): the FP64 factors rounded to float.
+template <int M>
+void tables_f32_m(std::vector<float> &tf) {
+    std::vector<double> tab;
+    tables_m<M>(tab);
+    constexpr int NT = M / kR, NS = FftPlan<M>::NS;
+    tf.assign(4 * (size_t)tw4_offset<M>(NS), 0.f);
+    auto pair = [&](int at4, int i0, int i1) {  // complex entries i0, i1 of the FP64 table (-1: zero pad)
+        float *o = &tf[4 * (size_t)at4];
+        if (i0 >= 0) o[0] = (float)tab[2 * i0], o[1] = (float)tab[2 * i0 + 1];
+        if (i1 >= 0) o[2] = (float)tab[2 * i1], o[3] = (float)tab[2 * i1 + 1];
+    };
+    for (int q = 0; q < kR / 2; q++)
+        for (int t = 0; t < NT; t++) pair(q * NT + t, (2 * q) * NT + t, (2 * q + 1) * NT + t);
+    for (int s = 1; s < NS; s++) {
+        const int L = stage_len<M>(s), r = FftPlan<M>::radix(s), st = L / r;
+        const int off = tw_offset<M>(s), off4 = tw4_offset<M>(s);
+        for (int q = 0; q < r / 2; q++)
+            for (int n1 = 0; n1 < st; n1++) {
+                const int k0 = 2 * q + 1, k1 = 2 * q + 2;
+                pair(off4 + q * st + n1, off + (k0 - 1) * st + n1, k1 < r ? off + (k1 - 1) * st + n1 : -1);
+            }
+    }
+}
+
 }  // namespace
 
 void fill_slot_freq(int N, std::vector<int32_t> &sf) {
@@ -278,6 +303,16 @@ void build_tables_fp64(int N, std::vector<double> &tab) {
         case 256: tables_m<256>(tab); break;
         case 512: tables_m<512>(tab); break;
         case 1024: tables_m<1024>(tab); break;
+        default: tab.clear();
+    }
+}
+
+void build_tables_f32(int N, std::vector<float> &tab) {
+    switch (N / 2) {
+        case 64: tables_f32_m<64>(tab); break;
+        case 256: tables_f32_m<256>(tab); break;
+        case 512: tables_f32_m<512>(tab); break;
+        case 1024: tables_f32_m<1024>(tab); break;
         default: tab.clear();
     }
 }

@@ -35,7 +35,7 @@ struct GateDesc {
 // Device-side FFT-domain bootstrapping key and tables for one precision.
 struct DeviceBsk {
     void *bsk = nullptr;      // [n][kpl][k+1][R][NT] x 16 bytes (double2, or float4 = hi.re,hi.im,lo.re,lo.im)
-    void *tables = nullptr;   // stage twiddles followed by the twist table [R][NT]
+    void *tables = nullptr;   // stage twiddles (stage 0 carries the twist), layout of the precision
     size_t bsk_bytes = 0;
     int split_shift = 0;      // split mode: weight of the high limb is 2^split_shift
 };
@@ -124,6 +124,7 @@ int32_t modswitch_from_torus32(int32_t phase, int32_t msize);
 
 // FFT-domain key preparation (host FP64), layout-compatible with the kernels.
 void build_tables_fp64(int N, std::vector<double> &tables);  // complex pairs (re,im)
+void build_tables_f32(int N, std::vector<float> &tables);    // float4 pairs of factors (tw4_offset)
 void fill_slot_freq(int N, std::vector<int32_t> &slot_freq); // [R][NT] -> frequency index
 // key_transform.cu: coefficient-domain bootstrapping key [n][kpl][k+1][N] on the device -> the
 // FFT-domain layout of `precision` (d_out: n*kpl*(k+1)*N/2*16 bytes), on stream s.
