@@ -1,0 +1,58 @@
+"""tfheb_gate_batch on host buffers against tfheb_gate_batch_device on the same inputs, bit for bit
+and decrypting to the truth table, for batches of several blind-rotation waves, a batch one gate
+above a wave, MUX, and a bootstrap-free gate; and the descriptor cache across calls of different
+sizes and gates."""
+import numpy as np
+import pytest
+
+import tfhe_b200 as tb
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TRUTH = {tb.api.NAND: lambda a, b, c: 1 - (a & b), tb.api.XOR: lambda a, b, c: a ^ b,
+         tb.api.MUX: lambda a, b, c: np.where(a == 1, b, c), tb.api.NOT: lambda a, b, c: 1 - a}
+
+
+@pytest.fixture(scope="module")
+def keys():
+    p = tb.default_params()
+    sk, ck = tb.keygen(p, seed=2024)
+    ck.to_device(0)
+    return p, sk, ck
+
+
+# 2500 NAND: several waves; 1500 MUX: 3000 bootstraps; 1037 XOR: one gate above a split-FP32 wave of
+# 148 x 7; 3000 NOT: no bootstrap
+@pytest.mark.parametrize("gate,count", [(tb.api.NAND, 2500), (tb.api.MUX, 1500), (tb.api.XOR, 1037),
+                                        (tb.api.NOT, 3000)])
+@pytest.mark.parametrize("precision", [tb.FP64, tb.SPLIT_FP32])
+def test_chunked_host_batch_equals_device_batch(keys, gate, count, precision):
+    p, sk, ck = keys
+    rng = np.random.default_rng(gate * 10 + precision)
+    bits = [rng.integers(0, 2, count) for _ in range(3)]
+    cts = [sk.encrypt(x, seed=30 + i) for i, x in enumerate(bits)]
+    binary = gate != tb.api.NOT
+    mux = gate == tb.api.MUX
+    host = ck.gate(gate, cts[0], cts[1] if binary else None, cts[2] if mux else None, precision=precision)
+    d = [torch.from_numpy(x).cuda() for x in cts]
+    d_out = torch.zeros_like(d[0])
+    ck.gate_device(gate, d[0], d[1] if binary else None, d[2] if mux else None, d_out, count, precision=precision)
+    ck.synchronize()
+    assert (host == d_out.cpu().numpy()).all()
+    got, _ = sk.decrypt(host)
+    assert (got == TRUTH[gate](*bits)).all()
+
+
+def test_descriptor_cache_across_sizes_and_gates(keys):
+    # descriptors built for a larger count serve a smaller one of the same gate (a prefix); another
+    # gate or a larger count rebuilds them
+    p, sk, ck = keys
+    rng = np.random.default_rng(3)
+    x, y, z = (rng.integers(0, 2, 600) for _ in range(3))
+    a, b, c = (sk.encrypt(v, seed=i) for i, v in enumerate((x, y, z)))
+    for gate, n in ((tb.api.NAND, 600), (tb.api.NAND, 37), (tb.api.MUX, 300), (tb.api.NAND, 599),
+                    (tb.api.MUX, 600)):
+        out = ck.gate(gate, a[:n], b[:n], c[:n] if gate == tb.api.MUX else None, precision=tb.SPLIT_FP32)
+        got, _ = sk.decrypt(out)
+        assert (got == TRUTH[gate](x[:n], y[:n], z[:n])).all(), (gate, n)

@@ -72,15 +72,10 @@ void gate_form(int gate, int32_t *cst, int32_t *sa, int32_t *sb) {
 
 // Builds bootstrap and gate descriptors for `count` gates with codes gates[g] (or a uniform code),
 // operands addressed by row indices (or the gate index itself when idx arrays are null).
-static void build_descs(int count, const int32_t *gates, int uniform, const int32_t *ia, const int32_t *ib,
-                        const int32_t *ic, std::vector<BootDesc> &bd, std::vector<GateDesc> &gd,
-                        std::vector<int32_t> *boot_rows) {
+static void build_descs(int count, const int32_t *gates, int uniform, std::vector<BootDesc> &bd,
+                        std::vector<GateDesc> &gd) {
     bd.clear();
     gd.assign(count, GateDesc{0, -1, 0});
-    (void)ia;
-    (void)ib;
-    (void)ic;
-    (void)boot_rows;
     const int32_t mu8 = modswitch_to_torus32(1, 8);
     for (int g = 0; g < count; g++) {
         const int code = gates ? gates[g] : uniform;
@@ -200,6 +195,41 @@ static tfheb_status upload_descs(CloudKey &ck, const std::vector<BootDesc> &bd, 
     return TFHEB_OK;
 }
 
+// Gate descriptors of `count` gates of one type.  They are per gate in batch order, so the array
+// built for a count serves every smaller count of the same gate (a prefix); it is rebuilt only for
+// another gate or a larger count.
+static tfheb_status ensure_descs(CloudKey &ck, int gate, int count, cudaStream_t s) {
+    if (ck.cached_gate == gate && count <= ck.cached_count) return TFHEB_OK;
+    std::vector<BootDesc> bd;
+    std::vector<GateDesc> gd;
+    build_descs(count, nullptr, gate, bd, gd);
+    const tfheb_status st = upload_descs(ck, bd, gd, s);
+    if (st != TFHEB_OK) return st;
+    ck.cached_gate = gate;
+    ck.cached_count = count;
+    return TFHEB_OK;
+}
+
+// `count` gates of one type on device buffers, enqueued on s (the key's lock held).
+static tfheb_status gate_chunk(CloudKey &ck, int gate, int precision, int count, const int32_t *d_a,
+                               const int32_t *d_b, const int32_t *d_c, int32_t *d_out, cudaStream_t s) {
+    const int n1 = ck.p.n + 1;
+    if (gate == TFHEB_COPY || gate == TFHEB_NOT) {
+        // bootstrap-free (boot-gates.cpp:164-178)
+        if (gate == TFHEB_COPY) {
+            TFHEB_CUDA(cudaMemcpyAsync(d_out, d_a, (size_t)count * n1 * 4, cudaMemcpyDeviceToDevice, s));
+            return TFHEB_OK;
+        }
+        TFHEB_CUDA(launch_negate(d_a, d_out, (size_t)count * n1, s));
+        g_launches += 1;
+        return TFHEB_OK;
+    }
+    const tfheb_status st = ensure_descs(ck, gate, count, s);
+    if (st != TFHEB_OK) return st;
+    const int boots = gate == TFHEB_MUX ? 2 * count : count;
+    return run_pipeline(ck, precision, count, boots, d_a, d_b, d_c, d_out, s);
+}
+
 }  // namespace tfheb
 
 using namespace tfheb;
@@ -308,7 +338,6 @@ void tfheb_cloud_key_free(tfheb_cloud_key *c) {
         cudaFree(ck.d_bdesc);
         cudaFree(ck.d_gdesc);
         cudaFree(ck.d_err);
-        if (ck.h_io) cudaFreeHost(ck.h_io);
         if (ck.stream) cudaStreamDestroy(ck.stream);
     }
     delete c;
@@ -450,57 +479,37 @@ tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *c, int32_t gate, int32_t p
     if (st != TFHEB_OK) return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
     if (count == 0) return TFHEB_OK;
-    const int n1 = ck.p.n + 1;
-    if (gate == TFHEB_COPY || gate == TFHEB_NOT) {
-        // bootstrap-free (boot-gates.cpp:164-178)
-        if (gate == TFHEB_COPY) {
-            TFHEB_CUDA(cudaMemcpyAsync(d_out, d_a, (size_t)count * n1 * 4, cudaMemcpyDeviceToDevice, s));
-            return TFHEB_OK;
-        }
-        TFHEB_CUDA(launch_negate(d_a, d_out, (size_t)count * n1, s));
-        g_launches += 1;
-        return TFHEB_OK;
-    }
-    if (ck.cached_gate != gate || ck.cached_count != count) {
-        std::vector<BootDesc> bd;
-        std::vector<GateDesc> gd;
-        build_descs(count, nullptr, gate, nullptr, nullptr, nullptr, bd, gd, nullptr);
-        if ((st = upload_descs(ck, bd, gd, s)) != TFHEB_OK) return st;
-        ck.cached_gate = gate;
-        ck.cached_count = count;
-    }
-    const int boots = gate == TFHEB_MUX ? 2 * count : count;
-    return run_pipeline(ck, precision, count, boots, d_a, d_b, d_c, d_out, s);
+    return gate_chunk(ck, gate, precision, count, d_a, d_b, d_c, d_out, s);
 }
 
+// Host buffers: inputs in, one launch sequence over the whole batch, output back, on the key's
+// stream.  Splitting a batch into wave-sized chunks whose copies overlap the neighbouring chunks'
+// gates gained nothing on B200 (102.4k NAND/s at 4096 split-FP32 gates, against 102.3k-103.9k
+// unsplit across boxes): the copies it hides (about 0.6 ms per 4096 gates) are offset by what the
+// chunks add, a keyswitch per chunk that streams the keyswitching key through L2 again and evicts
+// part of the bootstrapping key, and a ramp and tail per blind-rotation launch.
 tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precision, int32_t count,
                               const int32_t *a, const int32_t *b, const int32_t *cc, int32_t *out) {
-    if (!c || count < 0 || !a || !out) return TFHEB_ERR_INVALID;
+    if (!c || count < 0 || gate < 0 || gate > TFHEB_COPY || !a || !out) return TFHEB_ERR_INVALID;
+    if ((gate == TFHEB_MUX && (!b || !cc)) || (gate < TFHEB_MUX && !b)) return TFHEB_ERR_INVALID;
     if (count == 0) return TFHEB_OK;
-    CloudKey &ck = c->ck;
-    if (ck.device < 0) {
-        set_error("cloud key is not on a device (call tfheb_cloud_key_to_device)");
-        return TFHEB_ERR_INVALID;
-    }
-    const size_t row = (size_t)ck.p.n + 1, sz = (size_t)count * row;
-    int32_t *dio;
-    {
-        std::lock_guard<std::mutex> lock(c->mu);
-        TFHEB_CUDA(cudaSetDevice(ck.device));
-        tfheb_status st = grow(ck.d_io, ck.io_cap, 4 * sz);
-        if (st != TFHEB_OK) return st;
-        dio = ck.d_io;
-        cudaStream_t s = ck.stream;
-        TFHEB_CUDA(cudaMemcpyAsync(dio, a, sz * 4, cudaMemcpyHostToDevice, s));
-        if (b) TFHEB_CUDA(cudaMemcpyAsync(dio + sz, b, sz * 4, cudaMemcpyHostToDevice, s));
-        if (cc) TFHEB_CUDA(cudaMemcpyAsync(dio + 2 * sz, cc, sz * 4, cudaMemcpyHostToDevice, s));
-    }
-    tfheb_status st = tfheb_gate_batch_device(c, gate, precision, count, dio, b ? dio + sz : nullptr,
-                                              cc ? dio + 2 * sz : nullptr, dio + 3 * sz, nullptr);
-    if (st != TFHEB_OK) return st;
     std::lock_guard<std::mutex> lock(c->mu);
-    TFHEB_CUDA(cudaMemcpyAsync(out, dio + 3 * sz, sz * 4, cudaMemcpyDeviceToHost, ck.stream));
-    TFHEB_CUDA(cudaStreamSynchronize(ck.stream));
+    CloudKey &ck = c->ck;
+    tfheb_status st = ensure_device(ck, precision);
+    if (st != TFHEB_OK) return st;
+    const size_t sz = (size_t)count * (ck.p.n + 1);
+    if ((st = grow(ck.d_io, ck.io_cap, 4 * sz)) != TFHEB_OK) return st;
+    int32_t *dio = ck.d_io;
+    cudaStream_t s = ck.stream;
+    TFHEB_CUDA(cudaMemcpyAsync(dio, a, sz * 4, cudaMemcpyHostToDevice, s));
+    if (b) TFHEB_CUDA(cudaMemcpyAsync(dio + sz, b, sz * 4, cudaMemcpyHostToDevice, s));
+    if (cc) TFHEB_CUDA(cudaMemcpyAsync(dio + 2 * sz, cc, sz * 4, cudaMemcpyHostToDevice, s));
+    st = gate_chunk(ck, gate, precision, count, dio, b ? dio + sz : nullptr, cc ? dio + 2 * sz : nullptr,
+                    dio + 3 * sz, s);
+    if (st == TFHEB_OK) TFHEB_CUDA(cudaMemcpyAsync(out, dio + 3 * sz, sz * 4, cudaMemcpyDeviceToHost, s));
+    const cudaError_t e = cudaStreamSynchronize(s);  // drain, also after an error
+    if (st != TFHEB_OK) return st;
+    TFHEB_CUDA(e);
     return check_device_error(ck);
 }
 

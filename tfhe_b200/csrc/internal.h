@@ -80,10 +80,8 @@ struct CloudKey {
     size_t acc_cap = 0;
     int32_t *d_ksin = nullptr;
     size_t ksin_cap = 0;
-    int32_t *d_io = nullptr;        // staging of host batches: a,b,c,out
+    int32_t *d_io = nullptr;        // device copies of host batches: a,b,c,out
     size_t io_cap = 0;
-    int32_t *h_io = nullptr;        // pinned host staging
-    size_t h_io_cap = 0;
     BootDesc *d_bdesc = nullptr;
     size_t bdesc_cap = 0;
     GateDesc *d_gdesc = nullptr;
