@@ -81,10 +81,9 @@ struct BrLayout {
     static constexpr size_t teams = tables + tables_bytes;
     static constexpr size_t team_acc = 4 * (size_t)KP1 * N;
     static constexpr size_t team_xbuf = ((size_t)Exch<T, M>::bytes + 15) / 16 * 16;  // one exchange buffer
-    // two alternating exchange buffers (one barrier per exchange) up to N = 1024; at N = 2048 the
-    // second buffer costs more in shared memory and register pressure than the barrier it saves
-    // (measured 78.3 vs 72.6 ms per 2048 split bootstraps)
-    static constexpr int xbufs = N >= 2048 ? 1 : 2;
+    // two alternating exchange buffers: one barrier per exchange (at N = 2048 with the per-exchange
+    // float2 maps: 69.5 ms per 2048 split bootstraps against 69.7-70.5 ms with one buffer)
+    static constexpr int xbufs = 2;
     static constexpr size_t team_buf = xbufs * team_xbuf;
     __host__ __device__ static size_t team_bytes(int nsteps) {
         return team_acc + team_buf + 16 * (((size_t)nsteps + 4 + 3) / 4);
