@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -24,7 +25,7 @@ struct LweBootstrappingKey {
 struct LweBootstrappingKeyFFT {
     tfheb_cloud_key *ck;
     int32_t n, kN;
-    int32_t on_device_mask;
+    std::atomic<int32_t> on_device_mask;  // precisions whose FFT-domain key is on the device
 };
 
 namespace {
@@ -36,7 +37,7 @@ namespace {
 
 std::mutex g_rng_mu;
 uint64_t g_rng_state = 0x243F6A8885A308D3ull;  // reseeded by tfhe_random_generator_setSeed
-int32_t g_precision = TFHEB_FP64;
+std::atomic<int32_t> g_precision{TFHEB_FP64};  // set by tfhe_b200_set_precision, read by every gate
 
 uint64_t next_seed() {
     std::lock_guard<std::mutex> lock(g_rng_mu);
@@ -95,14 +96,20 @@ TFheGateBootstrappingSecretKeySet *assemble_secret_keyset(const TFheGateBootstra
     return make(TFheGateBootstrappingSecretKeySet{params, lk, new TGswKey{sk}, assemble_cloud(params, ck)});
 }
 
+// Moves the key of the current precision to the device on first use.  Threads may race here on a
+// fresh keyset: the transfer runs under the key's own lock and skips a precision already present,
+// so a second caller only waits; the mask is atomic.
+void ensure_on_device(LweBootstrappingKeyFFT *f) {
+    const int32_t bit = 1 << g_precision;
+    if (f->on_device_mask.load(std::memory_order_acquire) & bit) return;
+    if (tfheb_cloud_key_to_device(f->ck, device_index(), bit, 0) != TFHEB_OK) die("moving the key to the GPU");
+    f->on_device_mask.fetch_or(bit, std::memory_order_release);
+}
+
 LweBootstrappingKeyFFT *ready(const TFheGateBootstrappingCloudKeySet *bk) {
     auto *f = const_cast<LweBootstrappingKeyFFT *>(bk->bkFFT);
     if (!f || !f->ck) die("cloud keyset has no key");
-    const int bit = 1 << g_precision;
-    if (!(f->on_device_mask & bit)) {
-        if (tfheb_cloud_key_to_device(f->ck, device_index(), bit, 0) != TFHEB_OK) die("moving the key to the GPU");
-        f->on_device_mask |= bit;
-    }
+    ensure_on_device(f);
     return f;
 }
 
@@ -322,11 +329,7 @@ Torus32 lwePhase(const LweSample *sample, const LweKey *key) {
 static void bootstrap_one(LweSample *result, const LweBootstrappingKeyFFT *bkc, Torus32 mu, const LweSample *x,
                           bool with_ks) {
     auto *f = const_cast<LweBootstrappingKeyFFT *>(bkc);
-    const int bit = 1 << g_precision;
-    if (!(f->on_device_mask & bit)) {
-        if (tfheb_cloud_key_to_device(f->ck, device_index(), bit, 0) != TFHEB_OK) die("moving the key to the GPU");
-        f->on_device_mask |= bit;
-    }
+    ensure_on_device(f);
     const int32_t n = f->n, out_n = with_ks ? f->n : f->kN;
     std::vector<int32_t> in(n + 1), out(out_n + 1);
     std::memcpy(in.data(), x->a, sizeof(int32_t) * n);
