@@ -56,3 +56,20 @@ def test_descriptor_cache_across_sizes_and_gates(keys):
         out = ck.gate(gate, a[:n], b[:n], c[:n] if gate == tb.api.MUX else None, precision=tb.SPLIT_FP32)
         got, _ = sk.decrypt(out)
         assert (got == TRUTH[gate](x[:n], y[:n], z[:n])).all(), (gate, n)
+
+
+def test_device_entry_points_reject_host_memory(keys):
+    # a host array given where device memory is expected is refused before any kernel runs
+    p, sk, ck = keys
+    a = sk.encrypt(np.array([1, 0, 1]), seed=1)
+    d = torch.from_numpy(a).cuda()
+    d_out = torch.zeros_like(d)
+    with pytest.raises(tb.api.TfhebError, match="d_b: not device memory"):
+        ck.gate_device(tb.api.NAND, d, a, None, d_out, 3)
+    with pytest.raises(tb.api.TfhebError, match="d_out: not device memory"):
+        ck.gate_device(tb.api.NAND, d, d, None, np.zeros_like(a), 3)
+    # the key is still usable afterwards
+    ck.gate_device(tb.api.NAND, d, d, None, d_out, 3)
+    ck.synchronize()
+    got, _ = sk.decrypt(d_out.cpu().numpy())
+    assert (got == [0, 1, 0]).all()

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "internal.h"
@@ -70,8 +71,8 @@ void gate_form(int gate, int32_t *cst, int32_t *sa, int32_t *sb) {
     *sb = f.sb;
 }
 
-// Builds bootstrap and gate descriptors for `count` gates with codes gates[g] (or a uniform code),
-// operands addressed by row indices (or the gate index itself when idx arrays are null).
+// Builds bootstrap and gate descriptors for `count` gates with codes gates[g] (or one uniform code);
+// gate g reads row g of each operand batch.
 static void build_descs(int count, const int32_t *gates, int uniform, std::vector<BootDesc> &bd,
                         std::vector<GateDesc> &gd) {
     bd.clear();
@@ -192,6 +193,24 @@ static tfheb_status upload_descs(CloudKey &ck, const std::vector<BootDesc> &bd, 
     TFHEB_CUDA(cudaMemcpyAsync(ck.d_bdesc, bd.data(), bd.size() * sizeof(BootDesc), cudaMemcpyHostToDevice, s));
     TFHEB_CUDA(cudaMemcpyAsync(ck.d_gdesc, gd.data(), gd.size() * sizeof(GateDesc), cudaMemcpyHostToDevice, s));
     TFHEB_CUDA(cudaStreamSynchronize(s));  // host vectors are pageable temporaries
+    return TFHEB_OK;
+}
+
+// A caller's buffer must be device (or managed) memory that the key's GPU can address: a host
+// pointer or another GPU's memory would fault inside the kernels instead of returning an error.
+tfheb_status check_device_ptr(const CloudKey &ck, const void *ptr, const char *what) {
+    if (!ptr) return TFHEB_OK;
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        set_error(std::string(what) + ": not a CUDA pointer");
+        return TFHEB_ERR_INVALID;
+    }
+    if (attr.type == cudaMemoryTypeManaged) return TFHEB_OK;
+    if (attr.type != cudaMemoryTypeDevice || attr.device != ck.device) {
+        set_error(std::string(what) + ": not device memory on the key's GPU (device " + std::to_string(ck.device) + ")");
+        return TFHEB_ERR_INVALID;
+    }
     return TFHEB_OK;
 }
 
@@ -479,6 +498,8 @@ tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *c, int32_t gate, int32_t p
     if (st != TFHEB_OK) return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
     if (count == 0) return TFHEB_OK;
+    for (auto [ptr, what] : {std::pair<const void *, const char *>{d_a, "d_a"}, {d_b, "d_b"}, {d_c, "d_c"}, {d_out, "d_out"}})
+        if ((st = check_device_ptr(ck, ptr, what)) != TFHEB_OK) return st;
     return gate_chunk(ck, gate, precision, count, d_a, d_b, d_c, d_out, s);
 }
 
@@ -513,15 +534,9 @@ tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precisio
     return check_device_error(ck);
 }
 
-tfheb_status tfheb_bootstrap_woks_device(tfheb_cloud_key *c, int32_t precision, int32_t mu, int32_t count,
-                                         const int32_t *d_in, int32_t *d_out, void *stream) {
-    if (!c || count < 0 || !d_in || !d_out) return TFHEB_ERR_INVALID;
-    std::lock_guard<std::mutex> lock(c->mu);
-    CloudKey &ck = c->ck;
-    tfheb_status st = ensure_device(ck, precision);
-    if (st != TFHEB_OK) return st;
-    if (count == 0) return TFHEB_OK;
-    cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+// Bootstraps without keyswitch of `count` samples (the key's lock held).
+static tfheb_status bootstrap_woks_locked(CloudKey &ck, int32_t precision, int32_t mu, int32_t count,
+                                          const int32_t *d_in, int32_t *d_out, cudaStream_t s) {
     const tfheb_params &p = ck.p;
     // identity combination: x = in, one bootstrap per sample, no MUX term
     std::vector<BootDesc> bd(count);
@@ -530,6 +545,7 @@ tfheb_status tfheb_bootstrap_woks_device(tfheb_cloud_key *c, int32_t precision, 
         bd[g] = BootDesc{g, 0, 1, 0, 0, 0};
         gd[g] = GateDesc{g, -1, 0};
     }
+    tfheb_status st;
     if ((st = upload_descs(ck, bd, gd, s)) != TFHEB_OK) return st;
     ck.cached_gate = ck.cached_count = -1;
     const int bs = bara_stride_of(p);
@@ -544,22 +560,38 @@ tfheb_status tfheb_bootstrap_woks_device(tfheb_cloud_key *c, int32_t precision, 
     return TFHEB_OK;
 }
 
+tfheb_status tfheb_bootstrap_woks_device(tfheb_cloud_key *c, int32_t precision, int32_t mu, int32_t count,
+                                         const int32_t *d_in, int32_t *d_out, void *stream) {
+    if (!c || count < 0 || !d_in || !d_out) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    tfheb_status st = ensure_device(ck, precision);
+    if (st != TFHEB_OK) return st;
+    if (count == 0) return TFHEB_OK;
+    if ((st = check_device_ptr(ck, d_in, "d_in")) != TFHEB_OK || (st = check_device_ptr(ck, d_out, "d_out")) != TFHEB_OK)
+        return st;
+    return bootstrap_woks_locked(ck, precision, mu, count, d_in, d_out, stream ? (cudaStream_t)stream : ck.stream);
+}
+
+// Bootstrap then keyswitch, under one hold of the key's lock: the intermediate samples live in the
+// key's scratch, which another call on the key could otherwise reallocate in between.
 tfheb_status tfheb_bootstrap_device(tfheb_cloud_key *c, int32_t precision, int32_t mu, int32_t count,
                                     const int32_t *d_in, int32_t *d_out, void *stream) {
     if (!c || count < 0 || !d_in || !d_out) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
     CloudKey &ck = c->ck;
-    int32_t *tmp;
-    {
-        std::lock_guard<std::mutex> lock(c->mu);
-        if (ck.device < 0) return TFHEB_ERR_INVALID;
-        TFHEB_CUDA(cudaSetDevice(ck.device));
-        tfheb_status st = grow(ck.d_ksin, ck.ksin_cap, (size_t)count * (ck.p.k * ck.p.N + 1));
-        if (st != TFHEB_OK) return st;
-        tmp = ck.d_ksin;
-    }
-    tfheb_status st = tfheb_bootstrap_woks_device(c, precision, mu, count, d_in, tmp, stream);
+    tfheb_status st = ensure_device(ck, precision);
     if (st != TFHEB_OK) return st;
-    return tfheb_keyswitch_device(c, count, tmp, d_out, stream);
+    if (!ck.dksk.rows) return TFHEB_ERR_INVALID;
+    if (count == 0) return TFHEB_OK;
+    if ((st = check_device_ptr(ck, d_in, "d_in")) != TFHEB_OK || (st = check_device_ptr(ck, d_out, "d_out")) != TFHEB_OK)
+        return st;
+    if ((st = grow(ck.d_ksin, ck.ksin_cap, (size_t)count * (ck.p.k * ck.p.N + 1))) != TFHEB_OK) return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+    if ((st = bootstrap_woks_locked(ck, precision, mu, count, d_in, ck.d_ksin, s)) != TFHEB_OK) return st;
+    TFHEB_CUDA(launch_keyswitch(ck, count, ck.d_ksin, ck.p.k * ck.p.N + 1, d_out, s));
+    g_launches += 1;
+    return TFHEB_OK;
 }
 
 tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *c, int32_t precision, int32_t count, int32_t nsteps,
@@ -571,6 +603,8 @@ tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *c, int32_t precision, in
     tfheb_status st = ensure_device(ck, precision);
     if (st != TFHEB_OK) return st;
     if (count == 0) return TFHEB_OK;
+    if ((st = check_device_ptr(ck, d_bara, "d_bara")) != TFHEB_OK || (st = check_device_ptr(ck, d_acc, "d_acc")) != TFHEB_OK)
+        return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
     // in place: acc_in == acc_out is safe (each team reads its row fully before writing it back)
     TFHEB_CUDA(launch_blind_rotate(ck.p, precision, ck.dbsk[precision], d_bara, nsteps, count, nsteps, 0, d_acc,
@@ -588,6 +622,9 @@ tfheb_status tfheb_keyswitch_device(tfheb_cloud_key *c, int32_t count, const int
     if (ck.device < 0 || !ck.dksk.rows) return TFHEB_ERR_INVALID;
     TFHEB_CUDA(cudaSetDevice(ck.device));
     if (count == 0) return TFHEB_OK;
+    tfheb_status st;
+    if ((st = check_device_ptr(ck, d_in, "d_in")) != TFHEB_OK || (st = check_device_ptr(ck, d_out, "d_out")) != TFHEB_OK)
+        return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
     TFHEB_CUDA(launch_keyswitch(ck, count, d_in, ck.p.k * ck.p.N + 1, d_out, s));
     g_launches += 1;

@@ -162,6 +162,9 @@ int bara_stride_for(const tfheb_params &p);
 // Reads and clears the key's device error word (after the work has finished): TFHEB_ERR_TIMEOUT when
 // a bounded device-side wait expired.
 tfheb_status check_device_error(CloudKey &ck);
+// TFHEB_ERR_INVALID (with a message) unless ptr is NULL, managed memory, or device memory on the
+// key's GPU.
+tfheb_status check_device_ptr(const CloudKey &ck, const void *ptr, const char *what);
 extern std::atomic<int64_t> g_kernel_launches;
 
 // ---- reference file format (io.cu) ----------------------------------------------------------

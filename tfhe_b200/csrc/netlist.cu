@@ -468,6 +468,7 @@ tfheb_status tfheb_netlist_run(tfheb_netlist *nl, int32_t precision, int32_t *d_
     CloudKey &ck = nl->ck->ck;
     tfheb_status st = prepare_device(ck, precision);
     if (st != TFHEB_OK) return st;
+    if ((st = check_device_ptr(ck, d_wires, "tfheb_netlist_run: d_wires")) != TFHEB_OK) return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
     int kernels = 0;
     if (!use_graph) {
@@ -534,6 +535,7 @@ tfheb_status tfheb_gate_batch_mixed_device(tfheb_cloud_key *c, int32_t precision
     tfheb_status st = prepare_device(ck, precision);
     if (st != TFHEB_OK) return st;
     if (count == 0) return TFHEB_OK;
+    if ((st = check_device_ptr(ck, d_wires, "tfheb_gate_batch_mixed_device: d_wires")) != TFHEB_OK) return st;
     const tfheb_params &p = ck.p;
     const int n1 = p.n + 1, kN1 = p.k * p.N + 1, bs = bara_stride_for(p);
     auto row_ok = [&](const int32_t *idx, int g) { return idx && idx[g] >= 0 && idx[g] < num_wires; };
