@@ -165,7 +165,11 @@ tfheb_status tfheb_gate_batch_multi(tfheb_cloud_key *const *cks, int32_t nkeys, 
                                     int32_t count, const int32_t *a, const int32_t *b, const int32_t *c,
                                     int32_t *out);
 
-/* Same on device buffers, enqueued on `stream` (a cudaStream_t, NULL = the key's stream). */
+/* Same on device buffers, enqueued on `stream` (a cudaStream_t, NULL = the key's stream).  Every
+ * buffer must be device (or managed) memory on the key's GPU (TFHEB_ERR_INVALID otherwise); this holds
+ * for all *_device calls below.  Calls on one key may use different streams: those that use the
+ * key's scratch (this one, the bootstrap calls, tfheb_gate_batch) run on the GPU in call order, each
+ * waiting on the device for the previous one, and a netlist's runs likewise. */
 tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *ck, int32_t gate, int32_t precision, int32_t count,
                                      const int32_t *d_a, const int32_t *d_b, const int32_t *d_c, int32_t *d_out,
                                      void *stream);

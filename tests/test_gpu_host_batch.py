@@ -73,3 +73,31 @@ def test_device_entry_points_reject_host_memory(keys):
     ck.synchronize()
     got, _ = sk.decrypt(d_out.cpu().numpy())
     assert (got == [0, 1, 0]).all()
+
+
+def test_calls_on_two_streams_use_the_key_scratch_in_order(keys):
+    # two batches on one key, issued back to back on two streams with no host synchronisation: the
+    # second waits on the device for the first to finish with the key's scratch
+    import ctypes
+    p, sk, ck = keys
+    rng = np.random.default_rng(11)
+    n = 1500
+    bits = [rng.integers(0, 2, n) for _ in range(4)]
+    cts = [torch.from_numpy(sk.encrypt(x, seed=50 + i)).cuda() for i, x in enumerate(bits)]
+    o1, o2 = torch.zeros_like(cts[0]), torch.zeros_like(cts[0])
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.synchronize()
+    ck.gate_device(tb.api.NAND, cts[0], cts[1], None, o1, n, precision=tb.SPLIT_FP32,
+                   stream=ctypes.c_void_p(s1.cuda_stream))
+    ck.gate_device(tb.api.XOR, cts[2], cts[3], None, o2, n, precision=tb.SPLIT_FP32,
+                   stream=ctypes.c_void_p(s2.cuda_stream))
+    torch.cuda.synchronize()
+    g1, _ = sk.decrypt(o1.cpu().numpy())
+    g2, _ = sk.decrypt(o2.cpu().numpy())
+    assert (g1 == 1 - (bits[0] & bits[1])).all()
+    assert (g2 == (bits[2] ^ bits[3])).all()
+    # and bit for bit what one stream gives
+    r1 = torch.zeros_like(o1)
+    ck.gate_device(tb.api.NAND, cts[0], cts[1], None, r1, n, precision=tb.SPLIT_FP32)
+    ck.synchronize()
+    assert torch.equal(r1, o1)

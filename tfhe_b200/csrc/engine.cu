@@ -214,6 +214,22 @@ tfheb_status check_device_ptr(const CloudKey &ck, const void *ptr, const char *w
     return TFHEB_OK;
 }
 
+// Calls that use the key's scratch (descriptors, rotation amounts, accumulators, extracted samples,
+// host-batch copies) may come on different streams; each waits on the device for the previous one
+// to finish with the scratch, then marks its own end, so they run in call order on the GPU.
+static tfheb_status scratch_begin(CloudKey &ck, cudaStream_t s) {
+    if (!ck.scratch_done) {
+        TFHEB_CUDA(cudaEventCreateWithFlags(&ck.scratch_done, cudaEventDisableTiming));
+        return TFHEB_OK;
+    }
+    TFHEB_CUDA(cudaStreamWaitEvent(s, ck.scratch_done, 0));
+    return TFHEB_OK;
+}
+static tfheb_status scratch_end(CloudKey &ck, cudaStream_t s) {
+    TFHEB_CUDA(cudaEventRecord(ck.scratch_done, s));
+    return TFHEB_OK;
+}
+
 // Gate descriptors of `count` gates of one type.  They are per gate in batch order, so the array
 // built for a count serves every smaller count of the same gate (a prefix); it is rebuilt only for
 // another gate or a larger count.
@@ -357,6 +373,7 @@ void tfheb_cloud_key_free(tfheb_cloud_key *c) {
         cudaFree(ck.d_bdesc);
         cudaFree(ck.d_gdesc);
         cudaFree(ck.d_err);
+        if (ck.scratch_done) cudaEventDestroy(ck.scratch_done);
         if (ck.stream) cudaStreamDestroy(ck.stream);
     }
     delete c;
@@ -500,7 +517,10 @@ tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *c, int32_t gate, int32_t p
     if (count == 0) return TFHEB_OK;
     for (auto [ptr, what] : {std::pair<const void *, const char *>{d_a, "d_a"}, {d_b, "d_b"}, {d_c, "d_c"}, {d_out, "d_out"}})
         if ((st = check_device_ptr(ck, ptr, what)) != TFHEB_OK) return st;
-    return gate_chunk(ck, gate, precision, count, d_a, d_b, d_c, d_out, s);
+    if ((st = scratch_begin(ck, s)) != TFHEB_OK) return st;
+    st = gate_chunk(ck, gate, precision, count, d_a, d_b, d_c, d_out, s);
+    const tfheb_status se = scratch_end(ck, s);
+    return st != TFHEB_OK ? st : se;
 }
 
 // Host buffers: inputs in, one launch sequence over the whole batch, output back, on the key's
@@ -522,12 +542,14 @@ tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precisio
     if ((st = grow(ck.d_io, ck.io_cap, 4 * sz)) != TFHEB_OK) return st;
     int32_t *dio = ck.d_io;
     cudaStream_t s = ck.stream;
+    if ((st = scratch_begin(ck, s)) != TFHEB_OK) return st;
     TFHEB_CUDA(cudaMemcpyAsync(dio, a, sz * 4, cudaMemcpyHostToDevice, s));
     if (b) TFHEB_CUDA(cudaMemcpyAsync(dio + sz, b, sz * 4, cudaMemcpyHostToDevice, s));
     if (cc) TFHEB_CUDA(cudaMemcpyAsync(dio + 2 * sz, cc, sz * 4, cudaMemcpyHostToDevice, s));
     st = gate_chunk(ck, gate, precision, count, dio, b ? dio + sz : nullptr, cc ? dio + 2 * sz : nullptr,
                     dio + 3 * sz, s);
     if (st == TFHEB_OK) TFHEB_CUDA(cudaMemcpyAsync(out, dio + 3 * sz, sz * 4, cudaMemcpyDeviceToHost, s));
+    if (st == TFHEB_OK) st = scratch_end(ck, s);
     const cudaError_t e = cudaStreamSynchronize(s);  // drain, also after an error
     if (st != TFHEB_OK) return st;
     TFHEB_CUDA(e);
@@ -570,7 +592,11 @@ tfheb_status tfheb_bootstrap_woks_device(tfheb_cloud_key *c, int32_t precision, 
     if (count == 0) return TFHEB_OK;
     if ((st = check_device_ptr(ck, d_in, "d_in")) != TFHEB_OK || (st = check_device_ptr(ck, d_out, "d_out")) != TFHEB_OK)
         return st;
-    return bootstrap_woks_locked(ck, precision, mu, count, d_in, d_out, stream ? (cudaStream_t)stream : ck.stream);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+    if ((st = scratch_begin(ck, s)) != TFHEB_OK) return st;
+    st = bootstrap_woks_locked(ck, precision, mu, count, d_in, d_out, s);
+    const tfheb_status se = scratch_end(ck, s);
+    return st != TFHEB_OK ? st : se;
 }
 
 // Bootstrap then keyswitch, under one hold of the key's lock: the intermediate samples live in the
@@ -588,10 +614,15 @@ tfheb_status tfheb_bootstrap_device(tfheb_cloud_key *c, int32_t precision, int32
         return st;
     if ((st = grow(ck.d_ksin, ck.ksin_cap, (size_t)count * (ck.p.k * ck.p.N + 1))) != TFHEB_OK) return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
-    if ((st = bootstrap_woks_locked(ck, precision, mu, count, d_in, ck.d_ksin, s)) != TFHEB_OK) return st;
-    TFHEB_CUDA(launch_keyswitch(ck, count, ck.d_ksin, ck.p.k * ck.p.N + 1, d_out, s));
-    g_launches += 1;
-    return TFHEB_OK;
+    if ((st = scratch_begin(ck, s)) != TFHEB_OK) return st;
+    st = bootstrap_woks_locked(ck, precision, mu, count, d_in, ck.d_ksin, s);
+    if (st == TFHEB_OK) {
+        const cudaError_t e = launch_keyswitch(ck, count, ck.d_ksin, ck.p.k * ck.p.N + 1, d_out, s);
+        if (e != cudaSuccess) st = cuda_fail(e, "launch_keyswitch");
+        g_launches += 1;
+    }
+    const tfheb_status se = scratch_end(ck, s);
+    return st != TFHEB_OK ? st : se;
 }
 
 tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *c, int32_t precision, int32_t count, int32_t nsteps,

@@ -82,6 +82,7 @@ struct CloudKey {
     size_t ksin_cap = 0;
     int32_t *d_io = nullptr;        // device copies of host batches: a,b,c,out
     size_t io_cap = 0;
+    cudaEvent_t scratch_done = nullptr;  // the last call using the scratch above finished with it
     BootDesc *d_bdesc = nullptr;
     size_t bdesc_cap = 0;
     GateDesc *d_gdesc = nullptr;

@@ -119,6 +119,9 @@ struct tfheb_netlist {
     int32_t *d_bara = nullptr, *d_acc = nullptr, *d_ksin = nullptr;
     std::map<std::pair<int, const int32_t *>, cudaGraphExec_t> graphs;
     std::map<std::pair<int, const int32_t *>, cudaGraph_t> graph_defs;
+    // runs may come on different streams: each waits on the device for the previous run to finish
+    // with the shared state above, then marks its own end
+    cudaEvent_t run_done = nullptr;
 };
 
 // A netlist sharded across cloud keys on several devices: one schedule per key and precision
@@ -382,6 +385,9 @@ cudaError_t build_schedule(int num_inputs, int num_gates, const int32_t *gates,
     return e;
 }
 
+tfheb_status netlist_enqueue_run(tfheb_netlist *nl, CloudKey &ck, int32_t precision, int32_t *d_wires,
+                                 int32_t use_graph, cudaStream_t s);
+
 // Earliest level of every wire (inputs 0, a gate 1 + its deepest input) and the level count; an
 // error message when a gate code is unknown or a gate reads a wire that is not earlier.
 std::string earliest_levels(int num_inputs, int num_gates, const int32_t *gates, const int32_t *in_a,
@@ -470,6 +476,24 @@ tfheb_status tfheb_netlist_run(tfheb_netlist *nl, int32_t precision, int32_t *d_
     if (st != TFHEB_OK) return st;
     if ((st = check_device_ptr(ck, d_wires, "tfheb_netlist_run: d_wires")) != TFHEB_OK) return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+    cudaError_t eo = nl->run_done ? cudaStreamWaitEvent(s, nl->run_done, 0)
+                                  : cudaEventCreateWithFlags(&nl->run_done, cudaEventDisableTiming);
+    if (eo != cudaSuccess) return nl_fail(std::string("tfheb_netlist_run: ") + cudaGetErrorString(eo), TFHEB_ERR_CUDA);
+    st = netlist_enqueue_run(nl, ck, precision, d_wires, use_graph, s);
+    eo = cudaEventRecord(nl->run_done, s);
+    if (st == TFHEB_OK && eo != cudaSuccess)
+        return nl_fail(std::string("tfheb_netlist_run: ") + cudaGetErrorString(eo), TFHEB_ERR_CUDA);
+    return st;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Evaluates the netlist on stream s: eagerly, or through the CUDA graph of (precision, d_wires),
+// capturing it on the first graph run.
+tfheb_status netlist_enqueue_run(tfheb_netlist *nl, CloudKey &ck, int32_t precision, int32_t *d_wires,
+                                 int32_t use_graph, cudaStream_t s) {
     int kernels = 0;
     if (!use_graph) {
         const cudaError_t e = enqueue_netlist(nl, ck, precision, d_wires, s, &kernels);
@@ -507,11 +531,16 @@ tfheb_status tfheb_netlist_run(tfheb_netlist *nl, int32_t precision, int32_t *d_
     return TFHEB_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
 void tfheb_netlist_free(tfheb_netlist *nl) {
     if (!nl) return;
     cudaSetDevice(nl->ck->ck.device);
     for (auto &kv : nl->graphs) cudaGraphExecDestroy(kv.second);
     for (auto &kv : nl->graph_defs) cudaGraphDestroy(kv.second);
+    if (nl->run_done) cudaEventDestroy(nl->run_done);
     for (auto &sc : nl->sched) sc.release();
     cudaFree(nl->d_wires);
     cudaFree(nl->d_bara);
