@@ -43,11 +43,13 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["nand", "netlist", "mux2048", "errors", "keyswitch"], default="nand",
+    ap.add_argument("--workload", choices=["nand", "netlist", "mux2048", "errors", "keyswitch", "dropin"],
+                    default="nand",
                     help="nand: the headline line (4096 NAND batches); the others print their own line: "
                          "netlist = seeded 200-level random circuit through a CUDA graph, mux2048 = 1024 MUX "
                          "at N=2048, errors = decryption-error count over 10^6 split-FP32 NAND gates, "
-                         "keyswitch = the three keyswitch kernels on --batch extracted samples")
+                         "keyswitch = the three keyswitch kernels on --batch extracted samples, dropin = "
+                         "one bootsNAND per call through include/tfhe.h from 1, 16 and 64 threads")
     ap.add_argument("--gates", type=int, default=1_000_000, help="gate count of --workload errors")
     return ap.parse_args()
 
@@ -188,6 +190,23 @@ def run_extra_workload(args):
         ck.set_keyswitch_kernel(0)
         out.update({"samples": B, "ms_per_call": times, "bit_identical": True,
                     "params": "n=630,N=1024,k=1,ks_t=8,ks_basebit=2"})
+    elif args.workload == "dropin":
+        # the reference's calling pattern: a C client (tests/c/dropin_bench.c) compiled against
+        # include/tfhe.h calls bootsNAND once per gate, from several threads on one keyset
+        libdir = os.path.join(ROOT, "tfhe_b200")
+        with tempfile.TemporaryDirectory() as tmp:
+            exe = os.path.join(tmp, "dropin_bench")
+            subprocess.check_call(["gcc", "-std=c99", "-D_POSIX_C_SOURCE=200809L", "-O2", "-I",
+                                   os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "c", "dropin_bench.c"),
+                                   "-o", exe, "-L", libdir, "-ltfhe_b200", f"-Wl,-rpath,{libdir}", "-lpthread"])
+            runs = []
+            for threads, per_thread in ((1, 40), (16, 40), (64, 24), (256, 16)):
+                res = subprocess.run([exe, "1", str(threads), str(per_thread)], capture_output=True, text=True,
+                                     timeout=900)
+                if res.returncode != 0:
+                    raise RuntimeError(f"dropin_bench failed: {res.stdout}{res.stderr}")
+                runs.append(json.loads(res.stdout.strip().splitlines()[-1]))
+        out.update({"form": "split-FP32", "api": "bootsNAND (include/tfhe.h), one gate per call", "runs": runs})
     print(json.dumps(out), flush=True)
 
 

@@ -230,13 +230,20 @@ tfheb_status tfheb_profile_read(tfheb_cloud_key *ck, double *ms, int64_t *launch
  * measured by a dependent-chain probe kernel: the CUDA-core roofline denominator. */
 tfheb_status tfheb_measure_fma_peak(int32_t device, int32_t precision, double *tflops);
 
-/* Blind-rotation launch variants compiled for ring degree N and a precision: bootstraps per CTA
- * (teams_per_cta) and key-ring depth; *count receives how many exist (arrays filled up to cap).
- * tfheb_set_br_variant picks one for a key; tfheb_autotune times them all on `boots` synthetic
- * bootstraps, keeps the fastest for the key, and writes each variant's time to ms[] (up to cap).
- * No reference counterpart (the reference has one CPU code path). */
+/* Blind-rotation launch variants an autotuner chooses from, for ring degree N, gadget length l = 3
+ * (the 128-bit and N = 2048 sets) and a precision: bootstraps per CTA (teams_per_cta) and key-ring
+ * depth; *count receives how many exist (arrays filled up to cap).  tfheb_cloud_key_br_variants
+ * lists them for a key's own parameter set (the 80-bit set has l = 2).  tfheb_set_br_variant picks
+ * one for a key; tfheb_autotune times them all on `boots` synthetic bootstraps, keeps the fastest
+ * for the key, and writes each variant's time to ms[] (up to cap).  It then times, for each g below
+ * the winner's bootstraps per CTA, every compiled variant that fits a full wave of SMs x g bootstraps
+ * and keeps the fastest for such one-wave batches (without autotuning, split-FP32 one-wave batches
+ * use the variant with the fewest bootstraps per CTA that fits, FP64 the tuned one).  Results never
+ * depend on the variant.  No reference counterpart (the reference has one CPU code path). */
 tfheb_status tfheb_br_variants(int32_t N, int32_t precision, int32_t *teams_per_cta, int32_t *ring_depth,
                                int32_t cap, int32_t *count);
+tfheb_status tfheb_cloud_key_br_variants(const tfheb_cloud_key *ck, int32_t precision, int32_t *teams_per_cta,
+                                         int32_t *ring_depth, int32_t cap, int32_t *count);
 tfheb_status tfheb_set_br_variant(tfheb_cloud_key *ck, int32_t precision, int32_t variant);
 tfheb_status tfheb_autotune(tfheb_cloud_key *ck, int32_t precision, int32_t boots, double *ms, int32_t cap);
 

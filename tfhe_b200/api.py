@@ -73,6 +73,7 @@ def lib():
         L.tfheb_test_stall_key_stream.argtypes = [_V, _I32]
         L.tfheb_fft_slot_order.argtypes = [_I32, _V]
         L.tfheb_br_variants.argtypes = [_I32, _I32, _V, _V, _I32, _V]
+        L.tfheb_cloud_key_br_variants.argtypes = [_V, _I32, _V, _V, _I32, _V]
         L.tfheb_set_br_variant.argtypes = [_V, _I32, _I32]
         L.tfheb_autotune.argtypes = [_V, _I32, _I32, _V, _I32]
         L.tfheb_set_keyswitch_kernel.argtypes = [_V, _I32]
@@ -251,9 +252,19 @@ class CloudKey:
     def keyswitch_device(self, d_in, d_out, count, stream=None):
         _check(lib().tfheb_keyswitch_device(self.h, count, _p(d_in), _p(d_out), stream), "tfheb_keyswitch_device")
 
+    def br_variants(self, precision):
+        """The autotuner's candidate variants for this key: (teams_per_cta, ring_depth) arrays."""
+        cnt = ctypes.c_int32()
+        G = np.zeros(16, np.int32)
+        D = np.zeros(16, np.int32)
+        _check(lib().tfheb_cloud_key_br_variants(self.h, precision, _p(G), _p(D), 16, ctypes.byref(cnt)),
+               "tfheb_cloud_key_br_variants")
+        return G[:cnt.value], D[:cnt.value]
+
     def autotune(self, precision, boots=4096):
-        """Times every compiled blind-rotation variant; returns [(teams_per_cta, ring_depth, ms)]."""
-        G, D = br_variants(self.params.N, precision)
+        """Times every candidate blind-rotation variant (and the small-batch ones, for one-wave
+        batches); returns [(teams_per_cta, ring_depth, ms)] of the candidates."""
+        G, D = self.br_variants(precision)
         ms = np.zeros(len(G), np.float64)
         _check(lib().tfheb_autotune(self.h, precision, boots, _p(ms), len(G)), "tfheb_autotune")
         return list(zip(G.tolist(), D.tolist(), ms.tolist()))

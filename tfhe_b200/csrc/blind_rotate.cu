@@ -370,35 +370,46 @@ int blind_rotate_supported(const tfheb_params &p) {
 }
 
 // Compiled launch variants: (ring degree, precision, bootstraps per CTA G, key-ring depth D).
-// Every variant's shared memory stays within 227 KB.  The first variant of a (N, precision) pair is
-// the default; tfheb_autotune times all of them on the device and keeps the fastest per key.
+// Every variant's shared memory stays within 227 KB.  Tuned variants are the autotuner's candidates:
+// the first of a (N, l, precision) triple is the default, and tfheb_autotune times all of them on the
+// device and keeps the fastest per key.  Small variants (few bootstraps per CTA) serve batches that
+// fit one wave of CTAs with fewer bootstraps per SM than the tuned variant would pack (see
+// launch_blind_rotate).
 struct BrVariant {
     int N, l, precision, G, D;
+    bool tuned;
     cudaError_t (*launch)(const BrArgs &, cudaStream_t);
 };
 static const BrVariant kBrVariants[] = {
-    {1024, 3, TFHEB_SPLIT_FP32, 7, 4, launch_g<float, 1024, 3, true, 7, 4>},
-    {1024, 3, TFHEB_SPLIT_FP32, 5, 4, launch_g<float, 1024, 3, true, 5, 4>},
-    {1024, 3, TFHEB_SPLIT_FP32, 4, 4, launch_g<float, 1024, 3, true, 4, 4>},
-    {1024, 3, TFHEB_FP64, 3, 4, launch_g<double, 1024, 3, false, 3, 4>},
-    {1024, 3, TFHEB_FP64, 4, 4, launch_g<double, 1024, 3, false, 4, 4>},
-    {1024, 3, TFHEB_FP64, 4, 6, launch_g<double, 1024, 3, false, 4, 6>},
-    {1024, 3, TFHEB_FP64, 2, 4, launch_g<double, 1024, 3, false, 2, 4>},
-    {2048, 3, TFHEB_SPLIT_FP32, 3, 3, launch_g<float, 2048, 3, true, 3, 3>},
-    {2048, 3, TFHEB_SPLIT_FP32, 2, 3, launch_g<float, 2048, 3, true, 2, 3>},
-    {2048, 3, TFHEB_FP64, 2, 3, launch_g<double, 2048, 3, false, 2, 3>},
-    {2048, 3, TFHEB_FP64, 1, 4, launch_g<double, 2048, 3, false, 1, 4>},
-    {512, 3, TFHEB_SPLIT_FP32, 8, 4, launch_g<float, 512, 3, true, 8, 4>},
-    {512, 3, TFHEB_FP64, 8, 4, launch_g<double, 512, 3, false, 8, 4>},
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 4, true, launch_g<float, 1024, 3, true, 7, 4>},
+    {1024, 3, TFHEB_SPLIT_FP32, 5, 4, true, launch_g<float, 1024, 3, true, 5, 4>},
+    {1024, 3, TFHEB_SPLIT_FP32, 4, 4, true, launch_g<float, 1024, 3, true, 4, 4>},
+    {1024, 3, TFHEB_SPLIT_FP32, 3, 4, false, launch_g<float, 1024, 3, true, 3, 4>},
+    {1024, 3, TFHEB_SPLIT_FP32, 2, 4, false, launch_g<float, 1024, 3, true, 2, 4>},
+    {1024, 3, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 3, true, 1, 4>},
+    {1024, 3, TFHEB_FP64, 3, 4, true, launch_g<double, 1024, 3, false, 3, 4>},
+    {1024, 3, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 3, false, 4, 4>},
+    {1024, 3, TFHEB_FP64, 4, 6, true, launch_g<double, 1024, 3, false, 4, 6>},
+    {1024, 3, TFHEB_FP64, 2, 4, true, launch_g<double, 1024, 3, false, 2, 4>},
+    {1024, 3, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 3, false, 1, 4>},
+    {2048, 3, TFHEB_SPLIT_FP32, 3, 3, true, launch_g<float, 2048, 3, true, 3, 3>},
+    {2048, 3, TFHEB_SPLIT_FP32, 2, 3, true, launch_g<float, 2048, 3, true, 2, 3>},
+    {2048, 3, TFHEB_SPLIT_FP32, 1, 3, false, launch_g<float, 2048, 3, true, 1, 3>},
+    {2048, 3, TFHEB_FP64, 2, 3, true, launch_g<double, 2048, 3, false, 2, 3>},
+    {2048, 3, TFHEB_FP64, 1, 4, true, launch_g<double, 2048, 3, false, 1, 4>},
+    {512, 3, TFHEB_SPLIT_FP32, 8, 4, true, launch_g<float, 512, 3, true, 8, 4>},
+    {512, 3, TFHEB_FP64, 8, 4, true, launch_g<double, 512, 3, false, 8, 4>},
     // the 80-bit parameter set (n = 500, l = 2, Bgbit = 10; tfhe_gate_bootstrapping.cpp:23-48)
-    {1024, 2, TFHEB_SPLIT_FP32, 7, 4, launch_g<float, 1024, 2, true, 7, 4>},
-    {1024, 2, TFHEB_FP64, 4, 4, launch_g<double, 1024, 2, false, 4, 4>},
+    {1024, 2, TFHEB_SPLIT_FP32, 7, 4, true, launch_g<float, 1024, 2, true, 7, 4>},
+    {1024, 2, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 2, true, 1, 4>},
+    {1024, 2, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 2, false, 4, 4>},
+    {1024, 2, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 2, false, 1, 4>},
 };
 
 int br_variants(int N, int l, int precision, int *G, int *D, int cap) {
     int n = 0;
     for (const auto &v : kBrVariants)
-        if (v.N == N && v.l == l && v.precision == precision) {
+        if (v.tuned && v.N == N && v.l == l && v.precision == precision) {
             if (n < cap) {
                 if (G) G[n] = v.G;
                 if (D) D[n] = v.D;
@@ -408,20 +419,76 @@ int br_variants(int N, int l, int precision, int *G, int *D, int cap) {
     return n;
 }
 
+static BrArgs br_args(const tfheb_params &p, const DeviceBsk &bsk, const int32_t *bara, int bara_stride, int boots,
+                      int nsteps, int32_t mu, const int32_t *acc_in, int32_t *acc_out, int32_t *d_err,
+                      int stall_producer, uint64_t timeout_ns) {
+    return BrArgs{bara, bara_stride, reinterpret_cast<const uint8_t *>(bsk.bsk), bsk.tables, acc_in, acc_out, boots,
+                  nsteps, mu, p.Bgbit, bsk.split_shift, d_err, timeout_ns, stall_producer};
+}
+
+int br_variant_count() { return (int)(sizeof(kBrVariants) / sizeof(kBrVariants[0])); }
+
+void br_variant_info(int g, int *N, int *l, int *precision, int *G, int *D, int *tuned) {
+    const BrVariant &v = kBrVariants[g];
+    if (N) *N = v.N;
+    if (l) *l = v.l;
+    if (precision) *precision = v.precision;
+    if (G) *G = v.G;
+    if (D) *D = v.D;
+    if (tuned) *tuned = v.tuned;
+}
+
+int br_tuned_global(int N, int l, int precision, int tuned) {
+    int seen = 0;
+    for (int g = 0; g < br_variant_count(); g++) {
+        const BrVariant &v = kBrVariants[g];
+        if (v.tuned && v.N == N && v.l == l && v.precision == precision && seen++ == tuned) return g;
+    }
+    return -1;
+}
+
+cudaError_t launch_blind_rotate_exact(const tfheb_params &p, int precision, const DeviceBsk &bsk, const int32_t *bara,
+                                      int bara_stride, int boots, int nsteps, int32_t mu, const int32_t *acc_in,
+                                      int32_t *acc_out, cudaStream_t s, int32_t *d_err, int stall_producer,
+                                      uint64_t timeout_ns, int global_index) {
+    if (boots <= 0) return cudaSuccess;
+    if (global_index < 0 || global_index >= br_variant_count()) return cudaErrorInvalidValue;
+    const BrVariant &v = kBrVariants[global_index];
+    if (v.N != p.N || v.l != p.l || v.precision != precision) return cudaErrorInvalidValue;
+    return v.launch(br_args(p, bsk, bara, bara_stride, boots, nsteps, mu, acc_in, acc_out, d_err, stall_producer,
+                            timeout_ns), s);
+}
+
 cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const DeviceBsk &bsk, const int32_t *bara,
                                 int bara_stride, int boots, int nsteps, int32_t mu, const int32_t *acc_in,
                                 int32_t *acc_out, cudaStream_t s, int32_t *d_err, int stall_producer,
-                                uint64_t timeout_ns, int variant) {
+                                uint64_t timeout_ns, const BrChoice &choice) {
     if (boots <= 0) return cudaSuccess;
-    BrArgs a{bara, bara_stride, reinterpret_cast<const uint8_t *>(bsk.bsk), bsk.tables, acc_in, acc_out, boots,
-             nsteps, mu, p.Bgbit, bsk.split_shift, d_err, timeout_ns, stall_producer};
-    int seen = 0;
-    for (const auto &v : kBrVariants)
-        if (v.N == p.N && v.l == p.l && v.precision == precision) {
-            if (seen == variant) return v.launch(a, s);
-            seen++;
+    int g = br_tuned_global(p.N, p.l, precision, choice.tuned);
+    if (g < 0) return cudaErrorInvalidValue;
+    // A batch that fits one wave of CTAs with fewer bootstraps per CTA than the tuned variant packs
+    // may run faster spread thinner: at the default parameters a lone split-FP32 team finishes its
+    // 630 steps in 2.9 ms, while seven sharing an SM take 9.3 ms, so 16 gates packed 7 per CTA onto 3
+    // SMs would wait for the busiest of them.
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        sms > 0) {
+        const int need = (boots + sms - 1) / sms;  // bootstraps per CTA for one wave
+        if (need < kBrVariants[g].G && need < kSmallNeeds) {
+            const int e = choice.small[need];
+            if (e >= 0 && e < br_variant_count()) {
+                g = e;
+            } else if (e == -2 && precision == TFHEB_SPLIT_FP32) {
+                for (int i = 0; i < br_variant_count(); i++) {
+                    const BrVariant &v = kBrVariants[i];
+                    if (v.N == p.N && v.l == p.l && v.precision == precision && v.G >= need && v.G < kBrVariants[g].G)
+                        g = i;
+                }
+            }
         }
-    return cudaErrorInvalidValue;
+    }
+    return launch_blind_rotate_exact(p, precision, bsk, bara, bara_stride, boots, nsteps, mu, acc_in, acc_out, s, d_err,
+                                     stall_producer, timeout_ns, g);
 }
 
 }  // namespace tfheb

@@ -10,6 +10,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <mutex>
 #include <vector>
 
@@ -22,10 +24,25 @@ struct TGswKey {
 struct LweBootstrappingKey {
     tfheb_cloud_key *ck;
 };
+// One single-gate call waiting to be evaluated (see run_combined).
+struct GateRequest {
+    int32_t gate;
+    LweSample *res;
+    const LweSample *a, *b, *c;
+    bool done;
+};
+
 struct LweBootstrappingKeyFFT {
     tfheb_cloud_key *ck;
     int32_t n, kN;
     std::atomic<int32_t> on_device_mask;  // precisions whose FFT-domain key is on the device
+    // single-gate calls from concurrent threads, combined into batches
+    std::mutex comb_mu;
+    std::condition_variable comb_cv;      // callers waiting for their results or their turn
+    std::condition_variable comb_arrive;  // the batch's leader gathering requests
+    std::vector<GateRequest *> comb_pending;
+    bool comb_busy;
+    size_t comb_last;  // requests in the previous batch
 };
 
 namespace {
@@ -113,6 +130,74 @@ LweBootstrappingKeyFFT *ready(const TFheGateBootstrappingCloudKeySet *bk) {
     return f;
 }
 
+// Evaluates a set of single-gate requests: one batch per gate code present.  Every request's
+// operands are copied before its group's results are written, so a result may alias its own operands.
+void evaluate_requests(LweBootstrappingKeyFFT *f, const std::vector<GateRequest *> &reqs) {
+    const int32_t n = f->n, row = n + 1;
+    for (int32_t code = 0; code < TFHEB_NOT; code++) {
+        std::vector<GateRequest *> grp;
+        for (GateRequest *r : reqs)
+            if (r->gate == code) grp.push_back(r);
+        if (grp.empty()) continue;
+        const size_t cnt = grp.size();
+        std::vector<int32_t> ha(cnt * row), hb(cnt * row), hc(code == TFHEB_MUX ? cnt * row : 0), out(cnt * row);
+        auto put = [&](std::vector<int32_t> &buf, size_t i, const LweSample *x) {
+            std::memcpy(&buf[i * row], x->a, sizeof(int32_t) * n);
+            buf[i * row + n] = x->b;
+        };
+        for (size_t i = 0; i < cnt; i++) {
+            put(ha, i, grp[i]->a);
+            put(hb, i, grp[i]->b);
+            if (code == TFHEB_MUX) put(hc, i, grp[i]->c);
+        }
+        if (tfheb_gate_batch(f->ck, code, g_precision, (int32_t)cnt, ha.data(), hb.data(),
+                             code == TFHEB_MUX ? hc.data() : nullptr, out.data()) != TFHEB_OK)
+            die("gate evaluation");
+        for (size_t i = 0; i < cnt; i++) {
+            std::memcpy(grp[i]->res->a, &out[i * row], sizeof(int32_t) * n);
+            grp[i]->res->b = out[i * row + n];
+            grp[i]->res->current_variance = 0.;
+        }
+    }
+}
+
+// Longest time a batch's leader waits for the callers of the previous batch to post their next
+// gates: about 5 % of one single-bootstrap launch.
+constexpr auto kGatherWait = std::chrono::microseconds(200);
+
+// One bootstrapped gate from one caller.  Calls from concurrent threads are combined: a caller
+// queues its request, and whichever caller finds no evaluation running becomes the leader: it takes
+// every queued request and evaluates them together (one batch per gate code, evaluate_requests)
+// while the others wait; when it is done, a caller whose request arrived meanwhile leads the next
+// batch.  Callers that just got their results need a moment to post their next gates, so a leader
+// with fewer requests than the previous batch had waits up to kGatherWait for them.  A lone caller
+// evaluates its own gate at once; N concurrent callers share one launch sequence.
+void run_combined(int32_t gate, LweSample *res, const LweSample *a, const LweSample *b, const LweSample *c,
+                  LweBootstrappingKeyFFT *f) {
+    GateRequest req{gate, res, a, b, c, false};
+    std::unique_lock<std::mutex> lk(f->comb_mu);
+    f->comb_pending.push_back(&req);
+    f->comb_arrive.notify_one();
+    while (!req.done) {
+        if (f->comb_busy) {
+            f->comb_cv.wait(lk);
+            continue;
+        }
+        f->comb_busy = true;
+        if (f->comb_pending.size() < f->comb_last)
+            f->comb_arrive.wait_for(lk, kGatherWait, [&] { return f->comb_pending.size() >= f->comb_last; });
+        f->comb_last = f->comb_pending.size();
+        std::vector<GateRequest *> batch;
+        batch.swap(f->comb_pending);
+        lk.unlock();
+        evaluate_requests(f, batch);  // aborts on failure, like the reference's gates
+        lk.lock();
+        for (GateRequest *r : batch) r->done = true;
+        f->comb_busy = false;
+        f->comb_cv.notify_all();
+    }
+}
+
 void pack(std::vector<int32_t> &buf, const LweSample *s, int32_t count, int32_t n) {
     buf.resize((size_t)count * (n + 1));
     for (int32_t g = 0; g < count; g++) {
@@ -141,6 +226,10 @@ void run_batch(int32_t gate, LweSample *res, const LweSample *a, const LweSample
         return;
     }
     LweBootstrappingKeyFFT *f = ready(bk);
+    if (count == 1) {
+        run_combined(gate, res, a, b, c, f);
+        return;
+    }
     std::vector<int32_t> ha, hb, hc, out((size_t)count * (n + 1));
     pack(ha, a, count, n);
     pack(hb, b, count, n);

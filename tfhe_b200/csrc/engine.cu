@@ -162,7 +162,7 @@ static tfheb_status run_pipeline(CloudKey &ck, int precision, int count, int boo
     TFHEB_CUDA(timed(ck, 1, s, [&] {
         return launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, boots, p.n,
                                    modswitch_to_torus32(1, 8), nullptr, ck.d_acc, s, ck.d_err, ck.stall_producer,
-                                   ck.wait_timeout_ns, ck.br_variant[precision]);
+                                   ck.wait_timeout_ns, ck.br[precision]);
     }));
     TFHEB_CUDA(timed(ck, 2, s, [&] { return launch_extract(p, ck.d_gdesc, count, ck.d_acc, ck.d_ksin, kN1, s); }));
     TFHEB_CUDA(timed(ck, 3, s, [&] {
@@ -576,7 +576,7 @@ static tfheb_status bootstrap_woks_locked(CloudKey &ck, int32_t precision, int32
     TFHEB_CUDA(launch_prologue(p, ck.d_bdesc, count, d_in, d_in, d_in, ck.d_bara, bs, s));
     TFHEB_CUDA(launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, count, p.n, mu, nullptr,
                                    ck.d_acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns,
-                                   ck.br_variant[precision]));
+                                   ck.br[precision]));
     TFHEB_CUDA(launch_extract(p, ck.d_gdesc, count, ck.d_acc, d_out, p.k * p.N + 1, s));
     g_launches += 3;
     return TFHEB_OK;
@@ -640,7 +640,7 @@ tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *c, int32_t precision, in
     // in place: acc_in == acc_out is safe (each team reads its row fully before writing it back)
     TFHEB_CUDA(launch_blind_rotate(ck.p, precision, ck.dbsk[precision], d_bara, nsteps, count, nsteps, 0, d_acc,
                                    d_acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns,
-                                   ck.br_variant[precision]));
+                                   ck.br[precision]));
     g_launches += 1;
     return TFHEB_OK;
 }
@@ -687,12 +687,19 @@ tfheb_status tfheb_br_variants(int32_t N, int32_t precision, int32_t *teams_per_
     return TFHEB_OK;
 }
 
+tfheb_status tfheb_cloud_key_br_variants(const tfheb_cloud_key *c, int32_t precision, int32_t *teams_per_cta,
+                                         int32_t *ring_depth, int32_t cap, int32_t *count) {
+    if (!c || !count || cap < 0) return TFHEB_ERR_INVALID;
+    *count = br_variants(c->ck.p.N, c->ck.p.l, precision, teams_per_cta, ring_depth, cap);
+    return TFHEB_OK;
+}
+
 tfheb_status tfheb_set_br_variant(tfheb_cloud_key *c, int32_t precision, int32_t variant) {
     if (!c || (precision != TFHEB_FP64 && precision != TFHEB_SPLIT_FP32)) return TFHEB_ERR_INVALID;
     if (variant < 0 || variant >= br_variants(c->ck.p.N, c->ck.p.l, precision, nullptr, nullptr, 0))
         return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
-    c->ck.br_variant[precision] = variant;
+    c->ck.br[precision].tuned = variant;
     return TFHEB_OK;
 }
 
@@ -710,6 +717,27 @@ tfheb_status tfheb_set_keyswitch_kernel(tfheb_cloud_key *c, int32_t which) {
 
 // Times every compiled blind-rotation variant on `boots` synthetic bootstraps (random rotation
 // amounts, the key's own bootstrapping key) and keeps the fastest for this key and precision.
+// Device time of one blind-rotation launch of compiled variant g over `boots` bootstraps (the second
+// of two runs; the first warms up).
+static tfheb_status time_variant(CloudKey &ck, int precision, int g, int boots, cudaEvent_t e0, cudaEvent_t e1,
+                                 float *ms) {
+    const tfheb_params &p = ck.p;
+    for (int rep = 0; rep < 2; rep++) {
+        TFHEB_CUDA(cudaEventRecord(e0, ck.stream));
+        TFHEB_CUDA(launch_blind_rotate_exact(p, precision, ck.dbsk[precision], ck.d_bara, bara_stride_of(p), boots, p.n,
+                                             modswitch_to_torus32(1, 8), nullptr, ck.d_acc, ck.stream, ck.d_err, 0,
+                                             ck.wait_timeout_ns, g));
+        TFHEB_CUDA(cudaEventRecord(e1, ck.stream));
+        TFHEB_CUDA(cudaEventSynchronize(e1));
+        TFHEB_CUDA(cudaEventElapsedTime(ms, e0, e1));
+    }
+    return TFHEB_OK;
+}
+
+// Times every tuned variant on `boots` synthetic bootstraps and keeps the fastest.  Then, for each
+// bootstraps-per-CTA need g below the winner's G, times every compiled variant with g <= G <= the
+// winner's on one full wave (SMs x g bootstraps) and records the fastest in the key's small-batch
+// table (BrChoice).
 tfheb_status tfheb_autotune(tfheb_cloud_key *c, int32_t precision, int32_t boots, double *ms_out, int32_t cap) {
     if (!c || boots <= 0) return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
@@ -718,42 +746,61 @@ tfheb_status tfheb_autotune(tfheb_cloud_key *c, int32_t precision, int32_t boots
     if (st != TFHEB_OK) return st;
     const tfheb_params &p = ck.p;
     const int bs = bara_stride_of(p);
-    if ((st = grow(ck.d_bara, ck.bara_cap, (size_t)boots * bs)) != TFHEB_OK) return st;
-    if ((st = grow(ck.d_acc, ck.acc_cap, (size_t)boots * (p.k + 1) * p.N)) != TFHEB_OK) return st;
-    std::vector<int32_t> bara((size_t)boots * bs);
+    int sms = 0;
+    TFHEB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ck.device));
+    const int most = std::max(boots, sms * (kSmallNeeds - 1));
+    if ((st = grow(ck.d_bara, ck.bara_cap, (size_t)most * bs)) != TFHEB_OK) return st;
+    if ((st = grow(ck.d_acc, ck.acc_cap, (size_t)most * (p.k + 1) * p.N)) != TFHEB_OK) return st;
+    std::vector<int32_t> bara((size_t)most * bs);
     uint64_t x = 0x9E3779B97F4A7C15ull;
     for (auto &v : bara) {
         x ^= x << 13; x ^= x >> 7; x ^= x << 17;
         v = (int32_t)(x % (uint64_t)(2 * p.N));
     }
     TFHEB_CUDA(cudaMemcpy(ck.d_bara, bara.data(), bara.size() * 4, cudaMemcpyHostToDevice));
+    struct Events {
+        cudaEvent_t a = nullptr, b = nullptr;
+        ~Events() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } ev;
+    TFHEB_CUDA(cudaEventCreate(&ev.a));
+    TFHEB_CUDA(cudaEventCreate(&ev.b));
     const int nv = br_variants(p.N, p.l, precision, nullptr, nullptr, 0);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
     int best = 0;
     float best_ms = 1e30f;
     for (int v = 0; v < nv; v++) {
         float ms = 0;
-        for (int rep = 0; rep < 2; rep++) {  // first run warms up
-            TFHEB_CUDA(cudaEventRecord(e0, ck.stream));
-            TFHEB_CUDA(launch_blind_rotate(p, precision, ck.dbsk[precision], ck.d_bara, bs, boots, p.n,
-                                           modswitch_to_torus32(1, 8), nullptr, ck.d_acc, ck.stream, ck.d_err, 0,
-                                           ck.wait_timeout_ns, v));
-            TFHEB_CUDA(cudaEventRecord(e1, ck.stream));
-            TFHEB_CUDA(cudaEventSynchronize(e1));
-            cudaEventElapsedTime(&ms, e0, e1);
-        }
+        if ((st = time_variant(ck, precision, br_tuned_global(p.N, p.l, precision, v), boots, ev.a, ev.b, &ms)) != TFHEB_OK)
+            return st;
         if (ms_out && v < cap) ms_out[v] = ms;
         if (ms < best_ms) {
             best_ms = ms;
             best = v;
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    BrChoice choice;
+    choice.tuned = best;
+    const int best_g = br_tuned_global(p.N, p.l, precision, best);
+    int best_G = 0;
+    br_variant_info(best_g, nullptr, nullptr, nullptr, &best_G, nullptr, nullptr);
+    for (int need = 1; need < best_G && need < kSmallNeeds; need++) {
+        float fastest = 1e30f;
+        for (int g = 0; g < br_variant_count(); g++) {
+            int N = 0, l = 0, prec = 0, G = 0;
+            br_variant_info(g, &N, &l, &prec, &G, nullptr, nullptr);
+            if (N != p.N || l != p.l || prec != precision || G < need || G > best_G) continue;
+            float ms = 0;
+            if ((st = time_variant(ck, precision, g, sms * need, ev.a, ev.b, &ms)) != TFHEB_OK) return st;
+            if (ms < fastest) {
+                fastest = ms;
+                choice.small[need] = g == best_g ? -1 : g;
+            }
+        }
+    }
     if ((st = check_device_error(ck)) != TFHEB_OK) return st;
-    ck.br_variant[precision] = best;
+    ck.br[precision] = choice;
     return TFHEB_OK;
 }
 

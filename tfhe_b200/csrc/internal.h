@@ -61,6 +61,18 @@ struct ParamMeta {
     double tlwe_alpha_max = 0.012467;
 };
 
+// Blind-rotation variant choice of a key for one precision.  `tuned` indexes the autotuner's
+// candidates of (N, l, precision).  A batch that fits one wave of CTAs with g < kSmallNeeds
+// bootstraps per CTA, fewer than the tuned variant packs, runs small[g] instead: a compiled variant
+// (index into the whole table, br_variant_info), -1 for the tuned one, or -2 for the default rule
+// (split-FP32: the variant with the fewest bootstraps per CTA that still fits one wave; FP64: the
+// tuned one).  tfheb_autotune fills small[] from one-wave timings.
+constexpr int kSmallNeeds = 8;
+struct BrChoice {
+    int tuned = 0;
+    int small[kSmallNeeds] = {-2, -2, -2, -2, -2, -2, -2, -2};
+};
+
 struct CloudKey {
     tfheb_params p{};
     ParamMeta meta;
@@ -91,7 +103,7 @@ struct CloudKey {
     int32_t *d_err = nullptr;       // device error word (bounded waits that ran out)
     uint64_t wait_timeout_ns = 1000000000ull;  // limit of every device-side wait
     int stall_producer = 0;         // test hook: the key-streaming warp issues nothing
-    int br_variant[2] = {0, 0};     // chosen blind-rotation launch variant per precision
+    BrChoice br[2];                 // blind-rotation launch variants per precision
     int launches = 0;               // kernels launched (for the bench's launch count)
     // optional per-kernel timing with CUDA events on the launching stream
     bool prof = false;
@@ -136,7 +148,17 @@ cudaError_t launch_prologue(const tfheb_params &p, const BootDesc *d_desc, int b
 cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const DeviceBsk &bsk, const int32_t *bara,
                                 int bara_stride, int boots, int nsteps, int32_t mu, const int32_t *acc_in,
                                 int32_t *acc_out, cudaStream_t s, int32_t *d_err, int stall_producer,
-                                uint64_t timeout_ns, int variant);
+                                uint64_t timeout_ns, const BrChoice &choice);
+// The same with one compiled variant given by its index into the whole table (for timing).
+cudaError_t launch_blind_rotate_exact(const tfheb_params &p, int precision, const DeviceBsk &bsk, const int32_t *bara,
+                                      int bara_stride, int boots, int nsteps, int32_t mu, const int32_t *acc_in,
+                                      int32_t *acc_out, cudaStream_t s, int32_t *d_err, int stall_producer,
+                                      uint64_t timeout_ns, int global_index);
+// Size of the whole compiled table and one entry's shape; tuned = an autotuner candidate.
+int br_variant_count();
+void br_variant_info(int global_index, int *N, int *l, int *precision, int *G, int *D, int *tuned);
+// Index into the whole table of the `tuned`-th autotuner candidate of (N, l, precision), or -1.
+int br_tuned_global(int N, int l, int precision, int tuned);
 // Launch variants compiled for (N, l, precision): count, and their (G, D) into the arrays (up to cap).
 int br_variants(int N, int l, int precision, int *G, int *D, int cap);
 cudaError_t launch_extract(const tfheb_params &p, const GateDesc *d_desc, int count, const int32_t *acc,

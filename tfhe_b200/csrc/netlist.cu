@@ -167,7 +167,7 @@ cudaError_t enqueue_level(const Schedule &sc, const Level &L, CloudKey &ck, int 
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         e = launch_blind_rotate(p, precision, ck.dbsk[precision], w.bara, bs, L.boots, p.n, modswitch_to_torus32(1, 8),
                                 nullptr, w.acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns,
-                                ck.br_variant[precision]);
+                                ck.br[precision]);
         if (e != cudaSuccess) return e;
         e = launch_extract(p, sc.d_gate + L.gate_off, L.gates, w.acc, w.ksin, kN1, s);
         if (e != cudaSuccess) return e;
@@ -214,7 +214,7 @@ int wave_bootstraps(const CloudKey &ck, int precision) {
     int sms = 0, G[16] = {0}, D[16] = {0};
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ck.device);
     const int nv = br_variants(ck.p.N, ck.p.l, precision, G, D, 16);
-    const int v = ck.br_variant[precision];
+    const int v = ck.br[precision].tuned;
     return std::max(1, sms) * (nv > 0 && v < nv ? G[v] : 1);
 }
 
@@ -630,7 +630,7 @@ tfheb_status tfheb_gate_batch_mixed_device(tfheb_cloud_key *c, int32_t precision
         if (e == cudaSuccess)
             e = launch_blind_rotate(p, precision, ck.dbsk[precision], static_cast<int32_t *>(buf[4]), bs, boots, p.n,
                                     mu8, nullptr, static_cast<int32_t *>(buf[5]), s, ck.d_err, ck.stall_producer,
-                                    ck.wait_timeout_ns, ck.br_variant[precision]);
+                                    ck.wait_timeout_ns, ck.br[precision]);
         if (e == cudaSuccess)
             e = launch_extract(p, static_cast<const GateDesc *>(buf[1]), nb, static_cast<int32_t *>(buf[5]),
                                static_cast<int32_t *>(buf[6]), kN1, s);

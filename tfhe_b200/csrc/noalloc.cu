@@ -136,7 +136,7 @@ extern "C" tfheb_status tfheb_gate_batch_device_noalloc(tfheb_cloud_key *c, int3
     if (e == cudaSuccess)
         e = launch_blind_rotate(p, precision, ck.dbsk[precision], bara, bs, boots, p.n, modswitch_to_torus32(1, 8),
                                 nullptr, acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns,
-                                ck.br_variant[precision]);
+                                ck.br[precision]);
     if (e == cudaSuccess) e = launch_extract(p, gd, count, acc, ksin, kN1, s);
     if (e == cudaSuccess) e = launch_keyswitch(ck, count, ksin, kN1, d_out, s);
     if (e != cudaSuccess) {
