@@ -130,18 +130,37 @@ def noise_default(ref, rng):
     keys.free()
 
 
-def main():
+def keyswitch_general(ref, rng):
+    # lweKeySwitch with a keyswitch shape other than the default's t=8, basebit=2 (t=4, basebit=3:
+    # 8 rows per digit position, a 12-bit decomposition), which only the general per-sample kernel
+    # serves.  N=1024 as above; n=8 keeps the keyswitching key at 1.2 MB.  Own generator, so that it
+    # can be regenerated alone.
+    rng = np.random.default_rng(20261203)
+    p = dict(n=8, N=1024, k=1, l=3, Bgbit=7, ks_t=4, ks_basebit=3)
+    keys = ref.keygen(custom=p, ks_stdev=2**-15, bk_stdev=2**-25, seed=78)
+    _, _, ksk, _ = keys.export(bsk=False)
+    ks_in = rng.integers(-2**31, 2**31, (40, p["k"] * p["N"] + 1), dtype=np.int64).astype(np.int32)
+    ks_in[0, :] = 0
+    ks_in[1, :] = -1
+    ks_out = keys.keyswitch(ks_in)
+    np.savez_compressed(os.path.join(HERE, "keyswitch_t4b3.npz"), params=np.array(list(p.values()), np.int32),
+                        ksk=ksk, ks_inputs=ks_in, ks_outputs=ks_out)
+    keys.free()
+
+
+GENERATORS = [numerics, decomposition, rotations, extraction, products, gates_small, noise_default,
+              keyswitch_general]
+
+
+def main(names):
+    """Writes every fixture, or only those whose generator is named on the command line."""
     ref = RefLib.load(required=True)
     rng = np.random.default_rng(20240601)
-    numerics(ref, rng)
-    decomposition(ref, rng)
-    rotations(ref, rng)
-    extraction(ref, rng)
-    products(ref, rng)
-    gates_small(ref, rng)
-    noise_default(ref, rng)
+    for gen in GENERATORS:
+        if not names or gen.__name__ in names:
+            gen(ref, rng)
     print("golden vectors written to", HERE)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

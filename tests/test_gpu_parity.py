@@ -71,6 +71,35 @@ def test_keyswitch_bit_exact_vs_reference_golden(golden_small):
     assert (host(out) == g["ks_outputs"]).all()
 
 
+def test_keyswitch_other_shape_bit_exact_vs_reference_golden():
+    # t=4, basebit=3: only the general per-sample kernel serves it; the tiled and register-key
+    # kernels are instantiated for t=8, basebit=2 and refuse
+    g = np.load(os.path.join(GOLDEN, "keyswitch_t4b3.npz"))
+    p = tb.make_params(*map(int, g["params"]))
+    bsk = np.zeros((p.n, (p.k + 1) * p.l, p.k + 1, p.N), np.int32)  # not used by the keyswitch
+    ck = tb.CloudKey.from_raw(p, bsk, g["ksk"]).to_device(0, precisions=(tb.FP64,))
+    x = g["ks_inputs"]
+    out = torch.zeros((len(x), p.n + 1), dtype=torch.int32, device="cuda")
+    ck.keyswitch_device(dev(x), out, len(x))
+    assert (host(out) == g["ks_outputs"]).all()
+    for which in (2, 3):
+        with pytest.raises(tb.api.TfhebError, match="no tiled keyswitch"):
+            ck.set_keyswitch_kernel(which)
+
+
+@pytest.mark.parametrize("precision", [tb.FP64, tb.SPLIT_FP32])
+def test_gates_with_other_keyswitch_shape(precision):
+    # the whole gate pipeline on the per-sample keyswitch (t=4, basebit=3)
+    p = tb.make_params(200, 1024, 1, 3, 7, 4, 3)
+    sk, ck = tb.keygen(p, seed=43)
+    ck.to_device(0)
+    rng = np.random.default_rng(44)
+    x, y = rng.integers(0, 2, 300), rng.integers(0, 2, 300)
+    out = ck.gate(tb.api.XOR, sk.encrypt(x, seed=1), sk.encrypt(y, seed=2), precision=precision)
+    got, _ = sk.decrypt(out)
+    assert (got == (x ^ y)).all()
+
+
 def test_keyswitch_bit_exact_vs_oracle_default(oracle, default_keys):
     p, sk, ck, bsk, ksk = default_keys
     rng = np.random.default_rng(1)

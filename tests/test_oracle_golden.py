@@ -93,6 +93,15 @@ def test_keyswitch_golden_bit_exact(oracle, golden_dir):
     assert (out == g["ks_outputs"]).all()
 
 
+def test_keyswitch_golden_other_shape_bit_exact(oracle, golden_dir):
+    # t=4, basebit=3 (the general keyswitch shape, tests/golden/keyswitch_t4b3.npz)
+    g = np.load(os.path.join(golden_dir, "keyswitch_t4b3.npz"))
+    p = dict(zip(("n", "N", "k", "l", "Bgbit", "ks_t", "ks_basebit"), map(int, g["params"])))
+    assert g["ksk"].shape == (p["k"] * p["N"], 4, 8, p["n"] + 1)
+    out = oracle.keyswitch(p, g["ksk"], g["ks_inputs"])
+    assert (out == g["ks_outputs"]).all()
+
+
 def test_gates_golden_decrypt_and_phase(oracle, golden_dir):
     g, p = small_keys(golden_dir)
     codes = g["gate_codes"]
