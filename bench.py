@@ -51,6 +51,9 @@ def parse():
                          "keyswitch = the three keyswitch kernels on --batch extracted samples, dropin = "
                          "one bootsNAND per call through include/tfhe.h from 1, 16 and 64 threads")
     ap.add_argument("--gates", type=int, default=1_000_000, help="gate count of --workload errors")
+    ap.add_argument("--ring", type=int, choices=[1024, 2048], default=1024,
+                    help="--workload errors: 1024 = split-FP32 NAND at the default parameters (batches of "
+                         "4096); 2048 = MUX at n=800, N=2048 in both forms (batches of 1024)")
     return ap.parse_args()
 
 
@@ -138,6 +141,28 @@ def run_extra_workload(args):
                          "errors": int((got != np.where(a == 1, b, c)).sum()), "autotune": tune}
         out.update({"params": "n=800,N=2048,k=1,l=3,Bgbit=8,ks_t=8,ks_basebit=2", "batch": B,
                     "split_shift": int(tb.api.lib().tfheb_default_split_shift(ctypes.byref(p)))})
+    elif args.workload == "errors" and args.ring == 2048:
+        # config 5: bootsMUX at n=800, N=2048, decryption errors over --gates gates per form
+        p = tb.large_params()
+        sk, ck = tb.keygen(p, seed=8)
+        ck.to_device(0)
+        B = 1024
+        rng = np.random.default_rng(12)
+        dout = torch.zeros((B, p.n + 1), dtype=torch.int32, device="cuda")
+        for prec, name in ((tb.SPLIT_FP32, "split"), (tb.FP64, "fp64")):
+            ck.autotune(prec, boots=2 * B)
+            t0, errors, done, batch = time.perf_counter(), 0, 0, 0
+            while done < args.gates:
+                bits = rng.integers(0, 2, (3, B))
+                d = [torch.from_numpy(sk.encrypt(bits[i], seed=3 * batch + i + 1)).cuda() for i in range(3)]
+                ck.gate_device(tb.api.MUX, d[0], d[1], d[2], dout, B, precision=prec, stream=sptr)
+                got, _ = sk.decrypt(dout.cpu().numpy())
+                errors += int((got != np.where(bits[0] == 1, bits[1], bits[2])).sum())
+                done += B
+                batch += 1
+            out[name] = {"gates": done, "decryption_errors": errors, "batches": batch,
+                         "wall_s": time.perf_counter() - t0}
+        out.update({"gate": "MUX", "params": "n=800,N=2048,k=1,l=3,Bgbit=8,ks_t=8,ks_basebit=2"})
     elif args.workload == "errors":
         p = tb.default_params()
         sk, ck = tb.keygen(p, seed=6)
