@@ -52,8 +52,8 @@ def parse():
                          "one bootsNAND per call through include/tfhe.h from 1, 16 and 64 threads")
     ap.add_argument("--gates", type=int, default=1_000_000, help="gate count of --workload errors")
     ap.add_argument("--ring", type=int, choices=[1024, 2048], default=1024,
-                    help="--workload errors: 1024 = split-FP32 NAND at the default parameters (batches of "
-                         "4096); 2048 = MUX at n=800, N=2048 in both forms (batches of 1024)")
+                    help="--workload errors: 1024 = NAND at the default parameters in the --form form "
+                         "(batches of 4096); 2048 = MUX at n=800, N=2048 in both forms (batches of 1024)")
     return ap.parse_args()
 
 
@@ -167,7 +167,8 @@ def run_extra_workload(args):
         p = tb.default_params()
         sk, ck = tb.keygen(p, seed=6)
         ck.to_device(0)
-        ck.autotune(tb.SPLIT_FP32, boots=4096)
+        prec = tb.SPLIT_FP32 if args.form == "split" else tb.FP64
+        ck.autotune(prec, boots=4096)
         B, total, errors, done = 4096, args.gates, 0, 0
         rng = np.random.default_rng(11)
         dout = torch.zeros((B, p.n + 1), dtype=torch.int32, device="cuda")
@@ -177,13 +178,13 @@ def run_extra_workload(args):
             bits = rng.integers(0, 2, (2, B))
             da = torch.from_numpy(sk.encrypt(bits[0], seed=2 * batch + 1)).cuda()
             db = torch.from_numpy(sk.encrypt(bits[1], seed=2 * batch + 2)).cuda()
-            ck.gate_device(tb.api.NAND, da, db, None, dout, B, precision=tb.SPLIT_FP32, stream=sptr)
+            ck.gate_device(tb.api.NAND, da, db, None, dout, B, precision=prec, stream=sptr)
             got, _ = sk.decrypt(dout.cpu().numpy())
             errors += int((got != 1 - (bits[0] & bits[1])).sum())
             done += B
             batch += 1
-        out.update({"form": "split-FP32", "gates": done, "decryption_errors": errors, "batches": batch,
-                    "wall_s": time.perf_counter() - t0})
+        out.update({"form": "split-FP32" if args.form == "split" else "FP64", "gates": done,
+                    "decryption_errors": errors, "batches": batch, "wall_s": time.perf_counter() - t0})
     elif args.workload == "keyswitch":
         # default parameters, --batch random extracted samples (dimension kN + 1); each kernel runs
         # --warmup untimed then --steps timed calls on this stream; outputs must agree bit for bit
