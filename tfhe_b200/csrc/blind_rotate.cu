@@ -85,9 +85,12 @@ struct BrLayout {
     // float2 maps: 69.5 ms per 2048 split bootstraps against 69.7-70.5 ms with one buffer)
     static constexpr int xbufs = 2;
     static constexpr size_t team_buf = xbufs * team_xbuf;
-    __host__ __device__ static size_t team_bytes(int nsteps) {
-        return team_acc + team_buf + 16 * (((size_t)nsteps + 4 + 3) / 4);
-    }
+    // the rotated accumulator polynomial being decomposed (N words), read once per digit, up to
+    // N = 1024; at N = 2048 it stays in registers (8 KB more per team would not fit beside the key
+    // ring at 3 bootstraps per CTA)
+    static constexpr bool rot_in_smem = N <= 1024;
+    static constexpr size_t team_rot = rot_in_smem ? 4 * (size_t)N : 0;
+    __host__ __device__ static size_t team_bytes(int) { return team_acc + team_buf + team_rot; }
     __host__ __device__ static size_t bytes(int nsteps) { return teams + G * team_bytes(nsteps); }
     static_assert(2 * D * 8 + 4 <= 128, "barrier block");
 };
@@ -184,11 +187,10 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
     unsigned char *tb = smem + Lay::teams + (size_t)team * Lay::team_bytes(args.nsteps);
     uint32_t *s_acc = reinterpret_cast<uint32_t *>(tb);
     ExchPair xp{tb + Lay::team_acc, Lay::xbufs == 2 ? (uint32_t)Lay::team_xbuf : 0u, 0u};
-    int32_t *s_bara = reinterpret_cast<int32_t *>(tb + Lay::team_acc + Lay::team_buf);
+    uint32_t *s_rot = reinterpret_cast<uint32_t *>(tb + Lay::team_acc + Lay::team_buf);
     const cplx<T> *s_tw = s_tab;
 
     const int32_t *my_bara = args.bara + (size_t)boot * args.bara_stride;
-    for (int i = t; i < args.nsteps; i += NT) s_bara[i] = my_bara[i];
     if (args.acc_in) {
         const uint32_t *src = reinterpret_cast<const uint32_t *>(args.acc_in) + (size_t)boot * KP1 * N;
         for (int i = t; i < KP1 * N; i += NT) s_acc[i] = src[i];
@@ -218,8 +220,10 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
     const T digit_bias = DigitConv<T>::base() + T(1 << (Bgbit - 1));
 
     int c = 0;  // key-row (chunk) counter, same sequence as the producer
+    int a_next = args.nsteps > 0 ? my_bara[0] : 0;  // rotation amounts, loaded one step ahead
     for (int step = 0; step < args.nsteps; step++) {
-        const int ai = s_bara[step] & (2 * N - 1);
+        const int ai = a_next & (2 * N - 1);
+        if (step + 1 < args.nsteps) a_next = my_bara[step + 1];
         // FP64: one accumulator spectrum per output polynomial.  Split: hi- and lo-limb spectra as
         // packed register pairs over the slots (2m, 2m+1).
         cplx<T> acc_hi[SPLIT ? 1 : KP1][kR];
@@ -242,12 +246,22 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
 #pragma unroll 1
         for (int u = 0; u < KP1; u++) {
             const uint32_t *poly = s_acc + u * N;
-            uint32_t x0[kR], x1[kR];
+            // (X^a - 1) * poly + offset, kept for the L digits: in the team's scratch (each thread
+            // its own words, so no barrier, and no registers held across the digits' transforms)
+            // or, where that does not fit, in registers
+            uint32_t x[Lay::rot_in_smem ? 1 : 2 * kR];
 #pragma unroll
             for (int r = 0; r < kR; r++) {
                 const int j = t + NT * r;
-                x0[r] = rot_minus_one<N>(poly, j, ai) + offset;
-                x1[r] = rot_minus_one<N>(poly, j + M, ai) + offset;
+                const uint32_t v0 = rot_minus_one<N>(poly, j, ai) + offset;
+                const uint32_t v1 = rot_minus_one<N>(poly, j + M, ai) + offset;
+                if constexpr (Lay::rot_in_smem) {
+                    s_rot[r * NT + t] = v0;
+                    s_rot[(kR + r) * NT + t] = v1;
+                } else {
+                    x[r] = v0;
+                    x[kR + r] = v1;
+                }
             }
 #pragma unroll 1
             for (int q = 0; q < L; q++, c++) {
@@ -255,8 +269,10 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                 cplx<T> z[kR];
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
-                    const T d0 = DigitConv<T>::conv((x0[r] >> shift) & maskBg, digit_bias);
-                    const T d1 = DigitConv<T>::conv((x1[r] >> shift) & maskBg, digit_bias);
+                    const uint32_t v0 = Lay::rot_in_smem ? s_rot[r * NT + t] : x[r];
+                    const uint32_t v1 = Lay::rot_in_smem ? s_rot[(kR + r) * NT + t] : x[kR + r];
+                    const T d0 = DigitConv<T>::conv((v0 >> shift) & maskBg, digit_bias);
+                    const T d1 = DigitConv<T>::conv((v1 >> shift) & maskBg, digit_bias);
                     z[r] = cplx<T>{d0, -d1};  // a_j - i a_{j+M}; the twist is folded into the FFT
                 }
                 F::forward(z, xp, s_tw, t, bar_id);
