@@ -19,9 +19,11 @@
 // Precision forms:
 //   FP64  (SPLIT=false): key row slot = double2 B_k / M; products rounded with the 1.5*2^52 addition
 //          (exact round-to-nearest for |x| < 2^51), reduced mod 2^32.
-//   split (SPLIT=true):  key coefficient c = hi * 2^S + lo (S from default_split_shift); slot =
-//          float4 (hi, lo) spectra / M; both limb products are rounded exactly and recombined as
-//          hi * 2^S + lo mod 2^32.
+//   split (SPLIT=true):  key coefficient c = hi * 2^S + lo (S from default_split_shift); per register
+//          pair (2m, 2m+1) and limb, float4 {re(2m), re(2m+1), im(2m), im(2m+1)} / M, one 16-byte load
+//          per packed multiply-accumulate.  The high-limb product sums round to their exact integers
+//          (S keeps their FP32 error far below 1/2); the low-limb sums round to the nearest integer of
+//          their FP32 value; the two recombine as hi * 2^S + lo mod 2^32.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
