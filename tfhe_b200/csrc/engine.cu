@@ -118,11 +118,13 @@ static tfheb_status ensure_device(CloudKey &ck, int precision) {
 
 tfheb_status prepare_device(CloudKey &ck, int precision) { return ensure_device(ck, precision); }
 
-// Weight 2^S of the high limb in split mode.  The high-limb product must round to the exact
-// integer: its FP32 error is ~4 * 2^-24 * rms(product) with
+// Weight 2^S of the high limb in split mode.  The high-limb product sums must round to the exact
+// integer.  Their FP32 error grows with
 //   rms(product) = sqrt(N*(k+1)*l) * (2^Bgbit/sqrt12) * (2^(32-S)/sqrt12),
-// so S is the smallest shift keeping rms(product) <= 2^18 (error sigma <= 1/64 limb unit, >30 sigma
-// from a wrong rounding).  Default parameters give S = 24, the N=2048 set S = 26.
+// so S is the smallest shift keeping rms(product) <= 2^18.  An FP32 model of the arithmetic then
+// puts the error sigma at 0.021-0.028 of a unit for the reference's parameter sets, so a wrong
+// rounding (an error above 1/2) is 18 or more sigma away.  Default parameters give S = 24, the
+// N=2048 set S = 26, the 80-bit set S = 27.
 int default_split_shift(const tfheb_params &p) {
     const double terms = std::sqrt((double)p.N * (p.k + 1) * p.l);
     const double digit_rms = std::ldexp(1.0, p.Bgbit) / std::sqrt(12.0);
