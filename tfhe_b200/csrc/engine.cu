@@ -508,9 +508,9 @@ tfheb_status tfheb_cloud_key_fft_download(const tfheb_cloud_key *c, int32_t prec
 tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *c, int32_t gate, int32_t precision, int32_t count,
                                      const int32_t *d_a, const int32_t *d_b, const int32_t *d_c, int32_t *d_out,
                                      void *stream) {
-    if (!c || count < 0 || gate < 0 || gate > TFHEB_COPY || !d_a || !d_out) return TFHEB_ERR_INVALID;
-    if (gate == TFHEB_MUX && (!d_b || !d_c)) return TFHEB_ERR_INVALID;
-    if (gate < TFHEB_MUX && !d_b) return TFHEB_ERR_INVALID;
+    if (!c || count < 0 || gate < 0 || gate > TFHEB_COPY) return TFHEB_ERR_INVALID;
+    if (count > 0 && (!d_a || !d_out || (gate == TFHEB_MUX && (!d_b || !d_c)) || (gate < TFHEB_MUX && !d_b)))
+        return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
     CloudKey &ck = c->ck;
     tfheb_status st = ensure_device(ck, precision);
@@ -533,9 +533,9 @@ tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *c, int32_t gate, int32_t p
 // part of the bootstrapping key, and a ramp and tail per blind-rotation launch.
 tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precision, int32_t count,
                               const int32_t *a, const int32_t *b, const int32_t *cc, int32_t *out) {
-    if (!c || count < 0 || gate < 0 || gate > TFHEB_COPY || !a || !out) return TFHEB_ERR_INVALID;
-    if ((gate == TFHEB_MUX && (!b || !cc)) || (gate < TFHEB_MUX && !b)) return TFHEB_ERR_INVALID;
+    if (!c || count < 0 || gate < 0 || gate > TFHEB_COPY) return TFHEB_ERR_INVALID;
     if (count == 0) return TFHEB_OK;
+    if (!a || !out || (gate == TFHEB_MUX && (!b || !cc)) || (gate < TFHEB_MUX && !b)) return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
     CloudKey &ck = c->ck;
     tfheb_status st = ensure_device(ck, precision);
