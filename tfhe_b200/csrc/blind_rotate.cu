@@ -87,14 +87,19 @@ struct BrLayout {
     // float2 maps: 69.5 ms per 2048 split bootstraps against 69.7-70.5 ms with one buffer)
     static constexpr int xbufs = 2;
     static constexpr size_t team_buf = xbufs * team_xbuf;
-    // the rotated accumulator polynomial being decomposed (N words), read once per digit, up to
-    // N = 1024; at N = 2048 it stays in registers (8 KB more per team would not fit beside the key
-    // ring at 3 bootstraps per CTA)
-    static constexpr bool rot_in_smem = N <= 1024;
+    // the rotated accumulator polynomial being decomposed (N words), read once per digit: kept in a
+    // per-team shared scratch when registers are tight (more than 256 threads per CTA, so at most 168
+    // registers each) and the scratch fits beside the key ring, else in registers.  A deeper ring
+    // measured faster than the scratch (36.15 ms per 4096 split bootstraps at G = 7, D = 6 without it,
+    // 36.6 ms at D = 4 with it), and a lone team with 255 registers runs slower with it.
+    static constexpr size_t kMaxSmem = 227 * 1024;
+    static constexpr bool rot_in_smem =
+        G * (N / 16) + 32 > 256 && teams + G * (team_acc + team_buf + 4 * (size_t)N) <= kMaxSmem;
     static constexpr size_t team_rot = rot_in_smem ? 4 * (size_t)N : 0;
     __host__ __device__ static size_t team_bytes(int) { return team_acc + team_buf + team_rot; }
     __host__ __device__ static size_t bytes(int nsteps) { return teams + G * team_bytes(nsteps); }
     static_assert(2 * D * 8 + 4 <= 128, "barrier block");
+    static_assert(teams + G * (team_acc + team_buf) <= kMaxSmem, "shared memory of the variant");
 };
 
 struct BrArgs {
@@ -399,6 +404,7 @@ struct BrVariant {
     cudaError_t (*launch)(const BrArgs &, cudaStream_t);
 };
 static const BrVariant kBrVariants[] = {
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 6, true, launch_g<float, 1024, 3, true, 7, 6>},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 4, true, launch_g<float, 1024, 3, true, 7, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 5, 4, true, launch_g<float, 1024, 3, true, 5, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 4, 4, true, launch_g<float, 1024, 3, true, 4, 4>},
