@@ -77,7 +77,7 @@ struct BrLayout {
     static constexpr int M = N / 2, NT = M / kR, KP1 = K + 1;
     static constexpr uint32_t chunk = (uint32_t)KP1 * M * 16;  // one key row (step, p): all v, all slots
     static constexpr size_t bars = 0;                           // full[D], empty[D], abort flag
-    static constexpr size_t ring = 128;
+    static constexpr size_t ring = (2 * D * 8 + 4 + 127) / 128 * 128;  // the barrier block, then the ring
     static constexpr size_t tables = ring + (size_t)D * chunk;
     static constexpr size_t tables_bytes = tw_table_bytes<T, M>();
     static constexpr size_t teams = tables + tables_bytes;
@@ -98,7 +98,7 @@ struct BrLayout {
     static constexpr size_t team_rot = rot_in_smem ? 4 * (size_t)N : 0;
     __host__ __device__ static size_t team_bytes(int) { return team_acc + team_buf + team_rot; }
     __host__ __device__ static size_t bytes(int nsteps) { return teams + G * team_bytes(nsteps); }
-    static_assert(2 * D * 8 + 4 <= 128, "barrier block");
+    static_assert(2 * D * 8 + 4 <= ring, "barrier block");
     static_assert(teams + G * (team_acc + team_buf) <= kMaxSmem, "shared memory of the variant");
 };
 
