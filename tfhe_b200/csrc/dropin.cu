@@ -33,16 +33,17 @@ struct GateRequest {
 };
 
 struct LweBootstrappingKeyFFT {
+    LweBootstrappingKeyFFT(tfheb_cloud_key *key, int32_t lwe_n, int32_t ext_n) : ck(key), n(lwe_n), kN(ext_n) {}
     tfheb_cloud_key *ck;
     int32_t n, kN;
-    std::atomic<int32_t> on_device_mask;  // precisions whose FFT-domain key is on the device
+    std::atomic<int32_t> on_device_mask{0};  // precisions whose FFT-domain key is on the device
     // single-gate calls from concurrent threads, combined into batches
     std::mutex comb_mu;
     std::condition_variable comb_cv;      // callers waiting for their results or their turn
     std::condition_variable comb_arrive;  // the batch's leader gathering requests
     std::vector<GateRequest *> comb_pending;
-    bool comb_busy;
-    size_t comb_last;  // requests in the previous batch
+    bool comb_busy = false;
+    size_t comb_last = 0;  // requests in the previous batch
 };
 
 namespace {
@@ -102,7 +103,7 @@ TFheGateBootstrappingParameterSet *make_params(const tfheb_params &p, double in_
 TFheGateBootstrappingCloudKeySet assemble_cloud(const TFheGateBootstrappingParameterSet *params, tfheb_cloud_key *ck) {
     const tfheb_params p = to_params(params);
     return TFheGateBootstrappingCloudKeySet{params, new LweBootstrappingKey{ck},
-                                            new LweBootstrappingKeyFFT{ck, p.n, p.k * p.N, 0}};
+                                            new LweBootstrappingKeyFFT(ck, p.n, p.k * p.N)};
 }
 TFheGateBootstrappingSecretKeySet *assemble_secret_keyset(const TFheGateBootstrappingParameterSet *params,
                                                           tfheb_secret_key *sk, tfheb_cloud_key *ck) {
@@ -455,7 +456,7 @@ static void bootstrap_coef(LweSample *result, const LweBootstrappingKey *bk, Tor
     if (!bk || !bk->ck) die("bootstrapping key is empty");
     tfheb_params p;
     tfheb_cloud_key_params(bk->ck, &p);
-    const LweBootstrappingKeyFFT view{bk->ck, p.n, p.k * p.N, 0};  // moves missing device keys once
+    const LweBootstrappingKeyFFT view(bk->ck, p.n, p.k * p.N);  // moves missing device keys once
     bootstrap_one(result, &view, mu, x, with_ks);
 }
 
