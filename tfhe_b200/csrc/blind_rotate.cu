@@ -411,9 +411,9 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_SPLIT_FP32, 3, 4, false, launch_g<float, 1024, 3, true, 3, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 2, 4, false, launch_g<float, 1024, 3, true, 2, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 3, true, 1, 4>},
-    {1024, 3, TFHEB_FP64, 3, 4, true, launch_g<double, 1024, 3, false, 3, 4>},
-    {1024, 3, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 3, false, 4, 4>},
     {1024, 3, TFHEB_FP64, 4, 6, true, launch_g<double, 1024, 3, false, 4, 6>},
+    {1024, 3, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 3, false, 4, 4>},
+    {1024, 3, TFHEB_FP64, 3, 4, true, launch_g<double, 1024, 3, false, 3, 4>},
     {1024, 3, TFHEB_FP64, 2, 4, true, launch_g<double, 1024, 3, false, 2, 4>},
     {1024, 3, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 3, false, 1, 4>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_g<float, 2048, 3, true, 2, 4>},
