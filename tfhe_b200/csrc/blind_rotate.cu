@@ -319,33 +319,39 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
 #pragma unroll
         for (int v = 0; v < KP1; v++) {
             uint32_t c0[kR], c1[kR];
-            {
+            // Split: the two limbs' inverse transforms side by side (two independent chains) where
+            // registers allow, at most 384 threads per CTA (168 registers each): 64.1 against 65.6 ms
+            // per 2048 bootstraps at N = 2048, G = 2; at 128 registers the pair spills and ran 0.9 %
+            // slower (G = 7), so there the limbs go one after the other.
+            constexpr bool kPairInverse = G * NT + 32 <= 384;
+            if constexpr (SPLIT && kPairInverse) {
+                cplx<T> zh[kR], zl[kR];
+#pragma unroll
+                for (int m = 0; m < kR / 2; m++) {
+                    zh[2 * m] = {acc_h[v][m].re.x, acc_h[v][m].im.x};
+                    zh[2 * m + 1] = {acc_h[v][m].re.y, acc_h[v][m].im.y};
+                    zl[2 * m] = {acc_l[v][m].re.x, acc_l[v][m].im.x};
+                    zl[2 * m + 1] = {acc_l[v][m].re.y, acc_l[v][m].im.y};
+                }
+                F::inverse_pair(zh, zl, xp, s_tw, t, bar_id);
+#pragma unroll
+                for (int r = 0; r < kR; r++) {  // (c_j - i c_{j+M}) of each limb
+                    c0[r] = (round_f32_mod32(zh[r].re) << args.split_shift) + (uint32_t)__float2ll_rn(zl[r].re);
+                    c1[r] = (round_f32_mod32(-zh[r].im) << args.split_shift) + (uint32_t)__float2ll_rn(-zl[r].im);
+                }
+            } else if constexpr (SPLIT) {
                 cplx<T> z[kR];
-                if constexpr (SPLIT) {
 #pragma unroll
-                    for (int m = 0; m < kR / 2; m++) {
-                        z[2 * m] = {acc_h[v][m].re.x, acc_h[v][m].im.x};
-                        z[2 * m + 1] = {acc_h[v][m].re.y, acc_h[v][m].im.y};
-                    }
-                } else {
-#pragma unroll
-                    for (int r = 0; r < kR; r++) z[r] = acc_hi[v][r];
+                for (int m = 0; m < kR / 2; m++) {
+                    z[2 * m] = {acc_h[v][m].re.x, acc_h[v][m].im.x};
+                    z[2 * m + 1] = {acc_h[v][m].re.y, acc_h[v][m].im.y};
                 }
                 F::inverse(z, xp, s_tw, t, bar_id);
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
-                    const cplx<T> w = z[r];  // (c_j - i c_{j+M})
-                    if constexpr (SPLIT) {
-                        c0[r] = round_f32_mod32(w.re) << args.split_shift;
-                        c1[r] = round_f32_mod32(-w.im) << args.split_shift;
-                    } else {
-                        c0[r] = round_f64_mod32(w.re);
-                        c1[r] = round_f64_mod32(-w.im);
-                    }
+                    c0[r] = round_f32_mod32(z[r].re) << args.split_shift;
+                    c1[r] = round_f32_mod32(-z[r].im) << args.split_shift;
                 }
-            }
-            if constexpr (SPLIT) {
-                cplx<T> z[kR];
 #pragma unroll
                 for (int m = 0; m < kR / 2; m++) {
                     z[2 * m] = {acc_l[v][m].re.x, acc_l[v][m].im.x};
@@ -354,9 +360,18 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                 F::inverse(z, xp, s_tw, t, bar_id);
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
-                    const cplx<T> w = z[r];
-                    c0[r] += (uint32_t)__float2ll_rn(w.re);
-                    c1[r] += (uint32_t)__float2ll_rn(-w.im);
+                    c0[r] += (uint32_t)__float2ll_rn(z[r].re);
+                    c1[r] += (uint32_t)__float2ll_rn(-z[r].im);
+                }
+            } else {
+                cplx<T> z[kR];
+#pragma unroll
+                for (int r = 0; r < kR; r++) z[r] = acc_hi[v][r];
+                F::inverse(z, xp, s_tw, t, bar_id);
+#pragma unroll
+                for (int r = 0; r < kR; r++) {
+                    c0[r] = round_f64_mod32(z[r].re);  // (c_j - i c_{j+M})
+                    c1[r] = round_f64_mod32(-z[r].im);
                 }
             }
             uint32_t *poly = s_acc + v * N;

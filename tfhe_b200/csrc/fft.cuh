@@ -489,6 +489,41 @@ struct TeamFft {
         }
     }
 
+    // Two independent inverse transforms, stage by stage side by side: each array goes through
+    // exactly the operations of inverse(), and the scheduler gets two dependency chains.  Every
+    // exchange uses both exchange buffers (one per array), so a barrier precedes the first stores (the
+    // other buffer may still be read by the previous exchange) and separates each exchange's loads
+    // from the next one's stores.  Needs two buffers (xp.stride != 0).
+    template <int S>
+    __device__ static __forceinline__ void inverse_pair_from(cplx<T> *x, cplx<T> *y, const ExchPair &xp,
+                                                             const cplx<T> *tw, int t, int bar_id) {
+        constexpr int r = Stage<M, S>::r;
+        twiddle<S, true>(x, tw, t);
+        twiddle<S, true>(y, tw, t);
+#pragma unroll
+        for (int c = 0; c < R / r; c++) {
+            dft<T, true, r>(x + c * r);
+            dft<T, true, r>(y + c * r);
+        }
+        if constexpr (S > 0) {
+            unsigned char *bx = xp.base, *by = xp.base + xp.stride;
+            store<S, S - 1>(x, bx, t);
+            store<S, S - 1>(y, by, t);
+            team_sync(bar_id, NT);
+            load<S - 1, S - 1>(x, bx, t);
+            load<S - 1, S - 1>(y, by, t);
+            if constexpr (S - 1 > 0) team_sync(bar_id, NT);
+            inverse_pair_from<S - 1>(x, y, xp, tw, t, bar_id);
+        }
+    }
+    __device__ static __forceinline__ void inverse_pair(cplx<T> *x, cplx<T> *y, ExchPair &xp, const cplx<T> *tw, int t,
+                                                        int bar_id) {
+        team_sync(bar_id, NT);
+        inverse_pair_from<NS - 1>(x, y, xp, tw, t, bar_id);
+        fold_consts<true>(x);
+        fold_consts<true>(y);
+    }
+
     // Folded negacyclic transform.  In: x[n2] = a_j - i a_{j+M} for j = t + NT*n2 (no twist applied).
     // Out: the M evaluation points in slot order.
     __device__ static __forceinline__ void forward(cplx<T> *x, ExchPair &xp, const cplx<T> *tw, int t, int bar_id) {
