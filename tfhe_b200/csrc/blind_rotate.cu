@@ -316,14 +316,33 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
         }
 
         // inverse transforms, exact rounding, accumulate (the key was pre-scaled by 1/M)
+        // Two independent inverse transforms side by side (two dependency chains for the scheduler)
+        // where registers allow, at most 384 threads per CTA (168 registers each): the split form's
+        // two limbs of one output (64.1 against 65.6 ms per 2048 bootstraps at N = 2048, G = 2), FP64's
+        // two outputs.  At 128 registers the pair spills and ran 0.9 % slower (split, G = 7), so there
+        // the transforms go one after the other.
+        constexpr bool kPairInverse = G * NT + 32 <= 384;
+        if constexpr (!SPLIT && kPairInverse && KP1 == 2) {
+            cplx<T> z0[kR], z1[kR];
+#pragma unroll
+            for (int r = 0; r < kR; r++) {
+                z0[r] = acc_hi[0][r];
+                z1[r] = acc_hi[1][r];
+            }
+            F::inverse_pair(z0, z1, xp, s_tw, t, bar_id);
+#pragma unroll
+            for (int r = 0; r < kR; r++) {
+                const int j = t + NT * r;
+                s_acc[j] += round_f64_mod32(z0[r].re);  // (c_j - i c_{j+M})
+                s_acc[j + M] += round_f64_mod32(-z0[r].im);
+                s_acc[N + j] += round_f64_mod32(z1[r].re);
+                s_acc[N + j + M] += round_f64_mod32(-z1[r].im);
+            }
+        }
 #pragma unroll
         for (int v = 0; v < KP1; v++) {
+            if constexpr (!SPLIT && kPairInverse && KP1 == 2) break;  // done above
             uint32_t c0[kR], c1[kR];
-            // Split: the two limbs' inverse transforms side by side (two independent chains) where
-            // registers allow, at most 384 threads per CTA (168 registers each): 64.1 against 65.6 ms
-            // per 2048 bootstraps at N = 2048, G = 2; at 128 registers the pair spills and ran 0.9 %
-            // slower (G = 7), so there the limbs go one after the other.
-            constexpr bool kPairInverse = G * NT + 32 <= 384;
             if constexpr (SPLIT && kPairInverse) {
                 cplx<T> zh[kR], zl[kR];
 #pragma unroll
