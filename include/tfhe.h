@@ -92,6 +92,10 @@ typedef struct TFheGateBootstrappingSecretKeySet {
 } TFheGateBootstrappingSecretKeySet;
 
 /* ---- tfhe_gate_bootstrapping_functions.h:14-89 --------------------------------------------- */
+/* The gate functions run on the GPU.  Like the reference's, they may be called from several host
+ * threads at once on one cloud keyset (each thread with its own results); single-gate calls that
+ * arrive together are evaluated as one batch, so throughput grows with the number of calling
+ * threads.  A result may alias an operand. */
 TFHE_B200_EXPORT TFheGateBootstrappingParameterSet *new_default_gate_bootstrapping_parameters(int32_t minimum_lambda);
 TFHE_B200_EXPORT TFheGateBootstrappingSecretKeySet *
 new_random_gate_bootstrapping_secret_keyset(const TFheGateBootstrappingParameterSet *params);
