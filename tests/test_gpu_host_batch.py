@@ -120,3 +120,25 @@ def test_small_batches_match_large_batches_bit_for_bit(keys, precision):
         assert (small == big[:20]).all() and (mid == big[:300]).all()
         got, _ = sk.decrypt(big)
         assert (got == 1 - (x & y)).all()
+
+
+@pytest.mark.parametrize("precision", [tb.FP64, tb.SPLIT_FP32])
+def test_every_tuned_variant_gives_the_same_bits(keys, precision):
+    # 1036 gates need 7 bootstraps per CTA for one wave, no fewer than any candidate packs, so no
+    # small-batch variant stands in: packing, ring depth and paired transforms must not change a bit
+    p, sk, ck = keys
+    rng = np.random.default_rng(120 + precision)
+    x, y = rng.integers(0, 2, 1036), rng.integers(0, 2, 1036)
+    a, b = sk.encrypt(x, seed=121), sk.encrypt(y, seed=122)
+    G, _ = ck.br_variants(precision)
+    outs = []
+    try:
+        for v in range(len(G)):
+            ck.set_br_variant(precision, v)
+            outs.append(ck.gate(tb.api.NAND, a, b, precision=precision))
+    finally:
+        ck.set_br_variant(precision, 0)
+    for o in outs[1:]:
+        assert (o == outs[0]).all()
+    got, _ = sk.decrypt(outs[0])
+    assert (got == 1 - (x & y)).all()

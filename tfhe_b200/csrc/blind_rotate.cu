@@ -250,78 +250,136 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                 for (int r = 0; r < kR; r++) acc_hi[v][r] = {T(0), T(0)};
         }
 
-#pragma unroll 1
-        for (int u = 0; u < KP1; u++) {
-            const uint32_t *poly = s_acc + u * N;
-            // (X^a - 1) * poly + offset, kept for the L digits: in the team's scratch (each thread
-            // its own words, so no barrier, and no registers held across the digits' transforms)
-            // or, where that does not fit, in registers
-            uint32_t x[Lay::rot_in_smem ? 1 : 2 * kR];
+        // Two independent transforms side by side (two dependency chains for the scheduler) where
+        // registers allow.  Inverse, at most 384 threads per CTA (168 registers each): the split form's
+        // two limbs of one output (64.1 against 65.6 ms per 2048 bootstraps at N = 2048, G = 2), FP64's
+        // two outputs.  At 128 registers the pair spills and ran 0.9 % slower (split, G = 7), so there
+        // the transforms go one after the other.  Forward, FP64 at most 256 threads (255 registers):
+        // the digits in chain order, two at a time, so every accumulator takes its products in the
+        // same order as one at a time; the inverse that follows must be a pair (it begins with a
+        // barrier).  One wave of 148 bootstraps at G = 1: 3.07 against 3.36 ms; at G = 3, 51.7 against
+        // 53.6 ms per 4096.  The split form ran slower paired (3.97 against 3.20 ms at G = 1).
+        constexpr bool kPairInverse = G * NT + 32 <= 384;
+        constexpr bool kPairForward =
+            !SPLIT && G * NT + 32 <= 256 && !Lay::rot_in_smem && KPL % 2 == 0 && kPairInverse && KP1 == 2;
+        // one digit's spectrum times key row c into the accumulators; frees the row's ring slot
+        auto accumulate = [&](const cplx<T> *z) {
+            const int s = c % D;
+            wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns, args.err);
+            const unsigned char *stage = smem + Lay::ring + (size_t)s * Lay::chunk;
+            if constexpr (SPLIT) {
+                // key row: [v][m][limb][t] x float4 {re(2m), re(2m+1), im(2m), im(2m+1)}
+#pragma unroll
+                for (int m = 0; m < kR / 2; m++) {
+                    const cpair zp = make_cpair(z[2 * m], z[2 * m + 1]);
+                    const float2 nzi = mul2(zp.im, make_float2(-1.f, -1.f));
+#pragma unroll
+                    for (int v = 0; v < KP1; v++) {
+                        const float4 *kp = reinterpret_cast<const float4 *>(
+                            stage + ((size_t)((v * (kR / 2) + m) * 2) * NT + t) * 16);
+                        cmac_pair(acc_h[v][m], zp, nzi, kp[0]);
+                        cmac_pair(acc_l[v][m], zp, nzi, kp[NT]);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < KP1; v++)
+#pragma unroll
+                    for (int r = 0; r < kR; r++) {
+                        const size_t off = ((size_t)(v * kR + r) * NT + t) * 16;
+                        const double2 b = *reinterpret_cast<const double2 *>(stage + off);
+                        cmac(acc_hi[v][r], z[r], cplx<T>{(T)b.x, (T)b.y});
+                    }
+            }
+            mbar_arrive(empty_bar(s));
+            c++;
+        };
+        // digit q of the words x[r] (a_j) and x[kR + r] (a_{j+M}), j = t + NT * r
+        auto decompose = [&](cplx<T> *z, const uint32_t *x, int q) {
+            const int shift = 32 - (q + 1) * Bgbit;
 #pragma unroll
             for (int r = 0; r < kR; r++) {
-                const int j = t + NT * r;
-                const uint32_t v0 = rot_minus_one<N>(poly, j, ai) + offset;
-                const uint32_t v1 = rot_minus_one<N>(poly, j + M, ai) + offset;
-                if constexpr (Lay::rot_in_smem) {
-                    s_rot[r * NT + t] = v0;
-                    s_rot[(kR + r) * NT + t] = v1;
-                } else {
-                    x[r] = v0;
-                    x[kR + r] = v1;
-                }
+                const T d0 = DigitConv<T>::conv((x[r] >> shift) & maskBg, digit_bias);
+                const T d1 = DigitConv<T>::conv((x[kR + r] >> shift) & maskBg, digit_bias);
+                z[r] = cplx<T>{d0, -d1};  // a_j - i a_{j+M}; the twist is folded into the FFT
             }
-#pragma unroll 1
-            for (int q = 0; q < L; q++, c++) {
-                const int shift = 32 - (q + 1) * Bgbit;
-                cplx<T> z[kR];
+        };
+
+        if constexpr (kPairForward) {
+            // every polynomial's (X^a - 1) * poly + offset in registers, then the digits two at a time
+            uint32_t xr[KP1][2 * kR];
+#pragma unroll
+            for (int u = 0; u < KP1; u++)
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
-                    const uint32_t v0 = Lay::rot_in_smem ? s_rot[r * NT + t] : x[r];
-                    const uint32_t v1 = Lay::rot_in_smem ? s_rot[(kR + r) * NT + t] : x[kR + r];
-                    const T d0 = DigitConv<T>::conv((v0 >> shift) & maskBg, digit_bias);
-                    const T d1 = DigitConv<T>::conv((v1 >> shift) & maskBg, digit_bias);
-                    z[r] = cplx<T>{d0, -d1};  // a_j - i a_{j+M}; the twist is folded into the FFT
+                    const int j = t + NT * r;
+                    xr[u][r] = rot_minus_one<N>(s_acc + u * N, j, ai) + offset;
+                    xr[u][kR + r] = rot_minus_one<N>(s_acc + u * N, j + M, ai) + offset;
                 }
-                F::forward(z, xp, s_tw, t, bar_id);
-
-                const int s = c % D;
-                wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns, args.err);
-                const unsigned char *stage = smem + Lay::ring + (size_t)s * Lay::chunk;
-                if constexpr (SPLIT) {
-                    // key row: [v][m][limb][t] x float4 {re(2m), re(2m+1), im(2m), im(2m+1)}
+#pragma unroll 1
+            for (int d = 0; d < KPL; d += 2) {
+                cplx<T> za[kR], zb[kR];
+                uint32_t x[2 * kR];
 #pragma unroll
-                    for (int m = 0; m < kR / 2; m++) {
-                        const cpair zp = make_cpair(z[2 * m], z[2 * m + 1]);
-                        const float2 nzi = mul2(zp.im, make_float2(-1.f, -1.f));
+                for (int i = 0; i < 2 * kR; i++) {  // polynomial d / L (selects, no local memory)
+                    x[i] = xr[0][i];
 #pragma unroll
-                        for (int v = 0; v < KP1; v++) {
-                            const float4 *kp = reinterpret_cast<const float4 *>(
-                                stage + ((size_t)((v * (kR / 2) + m) * 2) * NT + t) * 16);
-                            cmac_pair(acc_h[v][m], zp, nzi, kp[0]);
-                            cmac_pair(acc_l[v][m], zp, nzi, kp[NT]);
-                        }
+                    for (int u = 1; u < KP1; u++)
+                        if (d / L == u) x[i] = xr[u][i];
+                }
+                decompose(za, x, d % L);
+#pragma unroll
+                for (int i = 0; i < 2 * kR; i++) {  // polynomial (d + 1) / L
+                    x[i] = xr[0][i];
+#pragma unroll
+                    for (int u = 1; u < KP1; u++)
+                        if ((d + 1) / L == u) x[i] = xr[u][i];
+                }
+                decompose(zb, x, (d + 1) % L);
+                F::forward_pair(za, zb, xp, s_tw, t, bar_id);
+                accumulate(za);
+                accumulate(zb);
+            }
+        } else {
+#pragma unroll 1
+            for (int u = 0; u < KP1; u++) {
+                const uint32_t *poly = s_acc + u * N;
+                // (X^a - 1) * poly + offset, kept for the L digits: in the team's scratch (each thread
+                // its own words, so no barrier, and no registers held across the digits' transforms)
+                // or, where that does not fit, in registers
+                uint32_t x[Lay::rot_in_smem ? 1 : 2 * kR];
+#pragma unroll
+                for (int r = 0; r < kR; r++) {
+                    const int j = t + NT * r;
+                    const uint32_t v0 = rot_minus_one<N>(poly, j, ai) + offset;
+                    const uint32_t v1 = rot_minus_one<N>(poly, j + M, ai) + offset;
+                    if constexpr (Lay::rot_in_smem) {
+                        s_rot[r * NT + t] = v0;
+                        s_rot[(kR + r) * NT + t] = v1;
+                    } else {
+                        x[r] = v0;
+                        x[kR + r] = v1;
                     }
-                } else {
-#pragma unroll
-                    for (int v = 0; v < KP1; v++)
-#pragma unroll
-                        for (int r = 0; r < kR; r++) {
-                            const size_t off = ((size_t)(v * kR + r) * NT + t) * 16;
-                            const double2 b = *reinterpret_cast<const double2 *>(stage + off);
-                            cmac(acc_hi[v][r], z[r], cplx<T>{(T)b.x, (T)b.y});
-                        }
                 }
-                mbar_arrive(empty_bar(s));
+#pragma unroll 1
+                for (int q = 0; q < L; q++) {
+                    const int shift = 32 - (q + 1) * Bgbit;
+                    cplx<T> z[kR];
+#pragma unroll
+                    for (int r = 0; r < kR; r++) {
+                        const uint32_t v0 = Lay::rot_in_smem ? s_rot[r * NT + t] : x[r];
+                        const uint32_t v1 = Lay::rot_in_smem ? s_rot[(kR + r) * NT + t] : x[kR + r];
+                        const T d0 = DigitConv<T>::conv((v0 >> shift) & maskBg, digit_bias);
+                        const T d1 = DigitConv<T>::conv((v1 >> shift) & maskBg, digit_bias);
+                        z[r] = cplx<T>{d0, -d1};  // a_j - i a_{j+M}; the twist is folded into the FFT
+                    }
+                    F::forward(z, xp, s_tw, t, bar_id);
+                    accumulate(z);
+                }
             }
         }
 
         // inverse transforms, exact rounding, accumulate (the key was pre-scaled by 1/M)
-        // Two independent inverse transforms side by side (two dependency chains for the scheduler)
-        // where registers allow, at most 384 threads per CTA (168 registers each): the split form's
-        // two limbs of one output (64.1 against 65.6 ms per 2048 bootstraps at N = 2048, G = 2), FP64's
-        // two outputs.  At 128 registers the pair spills and ran 0.9 % slower (split, G = 7), so there
-        // the transforms go one after the other.
-        constexpr bool kPairInverse = G * NT + 32 <= 384;
         if constexpr (!SPLIT && kPairInverse && KP1 == 2) {
             cplx<T> z0[kR], z1[kR];
 #pragma unroll
@@ -528,7 +586,8 @@ cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const Devi
     // A batch that fits one wave of CTAs with fewer bootstraps per CTA than the tuned variant packs
     // may run faster spread thinner: at the default parameters a lone split-FP32 team finishes its
     // 630 steps in 2.9 ms, while seven sharing an SM take 9.3 ms, so 16 gates packed 7 per CTA onto 3
-    // SMs would wait for the busiest of them.
+    // SMs would wait for the busiest of them.  FP64: 148 gates in 3.1 ms one per CTA, 7.3 ms four per
+    // CTA.
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
         sms > 0) {
@@ -537,7 +596,7 @@ cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const Devi
             const int e = choice.small[need];
             if (e >= 0 && e < br_variant_count()) {
                 g = e;
-            } else if (e == -2 && precision == TFHEB_SPLIT_FP32) {
+            } else if (e == -2) {
                 for (int i = 0; i < br_variant_count(); i++) {
                     const BrVariant &v = kBrVariants[i];
                     if (v.N == p.N && v.l == p.l && v.precision == precision && v.G >= need && v.G < kBrVariants[g].G)

@@ -489,6 +489,40 @@ struct TeamFft {
         }
     }
 
+    // Two independent forward transforms side by side, the counterpart of inverse_pair below (same
+    // barriers, both buffers, parity untouched): each array goes through exactly the operations of
+    // forward().  The caller's next exchange must begin with a barrier (forward_pair and
+    // inverse_pair do).
+    template <int S>
+    __device__ static __forceinline__ void forward_pair_from(cplx<T> *x, cplx<T> *y, const ExchPair &xp,
+                                                             const cplx<T> *tw, int t, int bar_id) {
+        constexpr int r = Stage<M, S>::r;
+#pragma unroll
+        for (int c = 0; c < R / r; c++) {
+            dft<T, false, r>(x + c * r);
+            dft<T, false, r>(y + c * r);
+        }
+        twiddle<S, false>(x, tw, t);
+        twiddle<S, false>(y, tw, t);
+        if constexpr (S + 1 < NS) {
+            unsigned char *bx = xp.base, *by = xp.base + xp.stride;
+            store<S, S>(x, bx, t);
+            store<S, S>(y, by, t);
+            team_sync(bar_id, NT);
+            load<S + 1, S>(x, bx, t);
+            load<S + 1, S>(y, by, t);
+            if constexpr (S + 2 < NS) team_sync(bar_id, NT);
+            forward_pair_from<S + 1>(x, y, xp, tw, t, bar_id);
+        }
+    }
+    __device__ static __forceinline__ void forward_pair(cplx<T> *x, cplx<T> *y, ExchPair &xp, const cplx<T> *tw, int t,
+                                                        int bar_id) {
+        fold_consts<false>(x);
+        fold_consts<false>(y);
+        team_sync(bar_id, NT);
+        forward_pair_from<0>(x, y, xp, tw, t, bar_id);
+    }
+
     // Two independent inverse transforms, stage by stage side by side: each array goes through
     // exactly the operations of inverse(), and the scheduler gets two dependency chains.  Every
     // exchange uses both exchange buffers (one per array), so a barrier precedes the first stores (the

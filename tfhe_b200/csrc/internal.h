@@ -65,8 +65,8 @@ struct ParamMeta {
 // candidates of (N, l, precision).  A batch that fits one wave of CTAs with g < kSmallNeeds
 // bootstraps per CTA, fewer than the tuned variant packs, runs small[g] instead: a compiled variant
 // (index into the whole table, br_variant_info), -1 for the tuned one, or -2 for the default rule
-// (split-FP32: the variant with the fewest bootstraps per CTA that still fits one wave; FP64: the
-// tuned one).  tfheb_autotune fills small[] from one-wave timings.
+// (the variant with the fewest bootstraps per CTA that still fits one wave).  tfheb_autotune fills
+// small[] from one-wave timings.
 constexpr int kSmallNeeds = 8;
 struct BrChoice {
     int tuned = 0;
