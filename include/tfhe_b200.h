@@ -237,9 +237,9 @@ tfheb_status tfheb_measure_fma_peak(int32_t device, int32_t precision, double *t
  * one for a key; tfheb_autotune times them all on `boots` synthetic bootstraps, keeps the fastest
  * for the key, and writes each variant's time to ms[] (up to cap).  It then times, for each g below
  * the winner's bootstraps per CTA, every compiled variant that fits a full wave of SMs x g bootstraps
- * and keeps the fastest for such one-wave batches (without autotuning, split-FP32 one-wave batches
- * use the variant with the fewest bootstraps per CTA that fits, FP64 the tuned one).  Results never
- * depend on the variant.  No reference counterpart (the reference has one CPU code path). */
+ * and keeps the fastest for such one-wave batches (without autotuning, one-wave batches use the
+ * variant with the fewest bootstraps per CTA that fits).  Results never depend on the variant.  No
+ * reference counterpart (the reference has one CPU code path). */
 tfheb_status tfheb_br_variants(int32_t N, int32_t precision, int32_t *teams_per_cta, int32_t *ring_depth,
                                int32_t cap, int32_t *count);
 tfheb_status tfheb_cloud_key_br_variants(const tfheb_cloud_key *ck, int32_t precision, int32_t *teams_per_cta,
