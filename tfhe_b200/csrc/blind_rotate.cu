@@ -466,6 +466,245 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
     for (int i = t; i < KP1 * N; i += NT) dst[i] = s_acc[i];
 }
 
+// ---- one bootstrap per CTA, digits in parallel ------------------------------------------------
+//
+// Latency form for batches far below one wave (a single drop-in gate, a few concurrent callers): one
+// CTA per bootstrap, one team per gadget digit ((k+1) * l teams of N/16 threads) plus the producer
+// warp.  Per step:
+//   1. team d rotates polynomial d / l, takes digit d % l and runs its forward transform; the spectra
+//      go to shared memory;
+//   2. jobs (output polynomial v, and in the split form the key limb) run on the first teams: the
+//      multiply-accumulate over the digits in order 0..(k+1)l-1 against the key rows, then the inverse
+//      transform, rounding and accumulation into the accumulator (split: the two limbs' teams add their
+//      parts with shared-memory atomics; integer sums mod 2^32 are order-free).
+// Each accumulator takes the same products in the same order as in blind_rotate_kernel, and each
+// transform runs the same operations, so the results are bit-identical to it.
+template <typename T, int N, int K, int L, int D, int XB>
+struct WideLayout {
+    static constexpr int M = N / 2, NT = M / kR, KP1 = K + 1, KPL = KP1 * L;
+    static constexpr uint32_t chunk = (uint32_t)KP1 * M * 16;
+    static constexpr size_t bars = 0;
+    static constexpr size_t ring = (2 * D * 8 + 4 + 127) / 128 * 128;
+    static constexpr size_t tables = ring + (size_t)D * chunk;
+    static constexpr size_t tables_bytes = tw_table_bytes<T, M>();
+    static constexpr size_t acc = (tables + tables_bytes + 127) / 128 * 128;
+    static constexpr size_t spec = acc + 4 * (size_t)KP1 * N;           // [digit][slot] spectra
+    static constexpr size_t spec_bytes = (size_t)KPL * M * 2 * sizeof(T);
+    static constexpr size_t xbuf_bytes = ((size_t)Exch<T, M>::bytes + 15) / 16 * 16;
+    static constexpr size_t xbufs = spec + spec_bytes;                   // [team][XB] exchange buffers
+    static constexpr size_t bytes = xbufs + (size_t)KPL * XB * xbuf_bytes;
+    static_assert(2 * D * 8 + 4 <= ring, "barrier block");
+    static_assert(bytes <= 227 * 1024, "shared memory of the variant");
+    static_assert(D >= 1 && (XB == 1 || XB == 2), "ring depth and exchange buffers");
+};
+
+template <typename T, int N, int K, int L, bool SPLIT, int D, int XB>
+__global__ void __launch_bounds__((K + 1) * L * (N / 16) + 32, 1) blind_rotate_wide_kernel(const BrArgs args) {
+    using Lay = WideLayout<T, N, K, L, D, XB>;
+    constexpr int M = N / 2, NT = M / kR, KP1 = K + 1, KPL = KP1 * L;
+    constexpr int JOBS = KP1 * (SPLIT ? 2 : 1);  // (output, limb) pairs
+    static_assert(JOBS <= KPL, "every job needs a team");
+    using F = TeamFft<T, M, kR>;
+    extern __shared__ __align__(128) unsigned char smem[];
+
+    const int tid = threadIdx.x;
+    constexpr int consumers = KPL * NT;
+    constexpr int kAllBar = 15;  // named barrier of all consumer teams (teams use 1..KPL)
+    static_assert(KPL < kAllBar, "named barrier ids");
+    const uint32_t bar0 = smem_addr(smem + Lay::bars);
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (D + s); };
+    volatile int32_t *abort_flag = reinterpret_cast<volatile int32_t *>(smem + Lay::bars + 16 * D);
+    const uint32_t ring = smem_addr(smem + Lay::ring);
+
+    if (tid == 0) {
+        for (int s = 0; s < D; s++) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), (uint32_t)(JOBS * NT));
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    {
+        const int4 *g_tab = reinterpret_cast<const int4 *>(args.tables);
+        int4 *s_tab4 = reinterpret_cast<int4 *>(smem + Lay::tables);
+        for (int i = tid; i < (int)(Lay::tables_bytes / 16); i += blockDim.x) s_tab4[i] = g_tab[i];
+    }
+    __syncthreads();
+
+    const int total_chunks = args.nsteps * KPL;
+    if (tid >= consumers) {  // producer warp: stream the key rows, as in blind_rotate_kernel
+        if (tid == consumers) {
+            int issued = 0;
+            if (!args.stall_producer) {
+                for (int c = 0; c < total_chunks; c++) {
+                    const int s = c % D;
+                    if (c >= D && !wait_bounded(empty_bar(s), ((c / D) - 1) & 1, abort_flag, args.timeout_ns, args.err))
+                        break;
+                    mbar_arrive_expect_tx(full_bar(s), Lay::chunk);
+                    bulk_copy_g2s(ring + (uint32_t)s * Lay::chunk, args.bsk + (size_t)c * Lay::chunk, Lay::chunk,
+                                  full_bar(s));
+                    issued = c + 1;
+                }
+            }
+            volatile int32_t no_abort = 0;
+            for (int c = (issued > D ? issued - D : 0); c < issued; c++)
+                wait_bounded(full_bar(c % D), (c / D) & 1, &no_abort, args.timeout_ns, args.err);
+        }
+        return;
+    }
+
+    const int team = tid / NT;  // digit of the forward phase; job of the accumulate phase
+    const int t = tid - team * NT;
+    const int bar_id = 1 + team;
+    const int boot = blockIdx.x;
+    uint32_t *s_acc = reinterpret_cast<uint32_t *>(smem + Lay::acc);
+    T *s_spec = reinterpret_cast<T *>(smem + Lay::spec);
+    ExchPair xp{smem + Lay::xbufs + (size_t)team * XB * Lay::xbuf_bytes, XB == 2 ? (uint32_t)Lay::xbuf_bytes : 0u,
+                0u};
+    const cplx<T> *s_tw = reinterpret_cast<const cplx<T> *>(smem + Lay::tables);
+
+    const int32_t *my_bara = args.bara + (size_t)boot * args.bara_stride;
+    if (args.acc_in) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(args.acc_in) + (size_t)boot * KP1 * N;
+        for (int i = tid; i < KP1 * N; i += consumers) s_acc[i] = src[i];
+    } else {
+        // acc = (0, X^{2N-barb} * [mu,...,mu])  (lwe-bootstrapping-functions-fft.cpp:142-145)
+        const int e = 2 * N - my_bara[args.nsteps];
+        for (int i = tid; i < K * N; i += consumers) s_acc[i] = 0u;
+        for (int j = tid; j < N; j += consumers) {
+            int src = j - e;
+            uint32_t neg = 0;
+            while (src < 0) {
+                src += N;
+                neg ^= 1u;
+            }
+            s_acc[K * N + j] = neg ? 0u - (uint32_t)args.mu : (uint32_t)args.mu;
+        }
+    }
+    team_sync(kAllBar, consumers);
+
+    // gadget constants (tgsw.cpp:7-29)
+    const int Bgbit = args.Bgbit;
+    uint32_t offset = 0;
+#pragma unroll
+    for (int q = 0; q < L; q++) offset += 1u << (32 - (q + 1) * Bgbit);
+    offset *= 1u << (Bgbit - 1);
+    const uint32_t maskBg = (1u << Bgbit) - 1u;
+    const T digit_bias = DigitConv<T>::base() + T(1 << (Bgbit - 1));
+    const int u_poly = team / L;                     // polynomial of this team's digit
+    const int shift = 32 - (team - u_poly * L + 1) * Bgbit;
+
+    int c = 0;  // first key row of the step
+    int a_next = args.nsteps > 0 ? my_bara[0] : 0;
+    for (int step = 0; step < args.nsteps; step++, c += KPL) {
+        const int ai = a_next & (2 * N - 1);
+        if (step + 1 < args.nsteps) a_next = my_bara[step + 1];
+
+        // 1. this team's digit: (X^a - 1) * poly + offset, digit, forward transform, spectrum out
+        {
+            const uint32_t *poly = s_acc + u_poly * N;
+            cplx<T> z[kR];
+#pragma unroll
+            for (int r = 0; r < kR; r++) {
+                const int j = t + NT * r;
+                const uint32_t v0 = rot_minus_one<N>(poly, j, ai) + offset;
+                const uint32_t v1 = rot_minus_one<N>(poly, j + M, ai) + offset;
+                const T d0 = DigitConv<T>::conv((v0 >> shift) & maskBg, digit_bias);
+                const T d1 = DigitConv<T>::conv((v1 >> shift) & maskBg, digit_bias);
+                z[r] = cplx<T>{d0, -d1};  // a_j - i a_{j+M}; the twist is folded into the FFT
+            }
+            F::forward(z, xp, s_tw, t, bar_id);
+            if constexpr (SPLIT) {
+                // [digit][m][t] float4 {re(2m), re(2m+1), im(2m), im(2m+1)}
+                float4 *sp = reinterpret_cast<float4 *>(s_spec) + (size_t)team * (kR / 2) * NT + t;
+#pragma unroll
+                for (int m = 0; m < kR / 2; m++)
+                    sp[m * NT] = make_float4(z[2 * m].re, z[2 * m + 1].re, z[2 * m].im, z[2 * m + 1].im);
+            } else {
+                double2 *sp = reinterpret_cast<double2 *>(s_spec) + (size_t)team * kR * NT + t;
+#pragma unroll
+                for (int r = 0; r < kR; r++) sp[r * NT] = make_double2(z[r].re, z[r].im);
+            }
+        }
+        team_sync(kAllBar, consumers);
+
+        // 2. job `team`: multiply-accumulate over the digits in order, inverse transform, accumulate
+        if (team < JOBS) {
+            const int v = SPLIT ? team >> 1 : team;
+            if constexpr (SPLIT) {
+                const int limb = team & 1;
+                cpair acc[kR / 2];
+#pragma unroll
+                for (int m = 0; m < kR / 2; m++) acc[m] = {{0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+                for (int d = 0; d < KPL; d++) {
+                    const int row = c + d, s = row % D;
+                    wait_bounded(full_bar(s), (row / D) & 1, abort_flag, args.timeout_ns, args.err);
+                    const float4 *kp = reinterpret_cast<const float4 *>(smem + Lay::ring + (size_t)s * Lay::chunk);
+                    const float4 *sp = reinterpret_cast<const float4 *>(s_spec) + (size_t)d * (kR / 2) * NT + t;
+#pragma unroll
+                    for (int m = 0; m < kR / 2; m++) {
+                        const float4 f = sp[m * NT];
+                        const cpair zp{{f.x, f.y}, {f.z, f.w}};
+                        const float2 nzi = mul2(zp.im, make_float2(-1.f, -1.f));
+                        cmac_pair(acc[m], zp, nzi, kp[((v * (kR / 2) + m) * 2 + limb) * NT + t]);
+                    }
+                    mbar_arrive(empty_bar(s));
+                }
+                cplx<T> z[kR];
+#pragma unroll
+                for (int m = 0; m < kR / 2; m++) {
+                    z[2 * m] = {acc[m].re.x, acc[m].im.x};
+                    z[2 * m + 1] = {acc[m].re.y, acc[m].im.y};
+                }
+                F::inverse(z, xp, s_tw, t, bar_id);
+                uint32_t *poly = s_acc + v * N;
+#pragma unroll
+                for (int r = 0; r < kR; r++) {  // (c_j - i c_{j+M}) of this limb
+                    const int j = t + NT * r;
+                    const uint32_t c0 = limb == 0 ? round_f32_mod32(z[r].re) << args.split_shift
+                                                  : (uint32_t)__float2ll_rn(z[r].re);
+                    const uint32_t c1 = limb == 0 ? round_f32_mod32(-z[r].im) << args.split_shift
+                                                  : (uint32_t)__float2ll_rn(-z[r].im);
+                    atomicAdd(poly + j, c0);
+                    atomicAdd(poly + j + M, c1);
+                }
+            } else {
+                cplx<T> acc[kR];
+#pragma unroll
+                for (int r = 0; r < kR; r++) acc[r] = {T(0), T(0)};
+#pragma unroll
+                for (int d = 0; d < KPL; d++) {
+                    const int row = c + d, s = row % D;
+                    wait_bounded(full_bar(s), (row / D) & 1, abort_flag, args.timeout_ns, args.err);
+                    const double2 *kp = reinterpret_cast<const double2 *>(smem + Lay::ring + (size_t)s * Lay::chunk);
+                    const double2 *sp = reinterpret_cast<const double2 *>(s_spec) + (size_t)d * kR * NT + t;
+#pragma unroll
+                    for (int r = 0; r < kR; r++) {
+                        const double2 zz = sp[r * NT];
+                        const double2 b = kp[(v * kR + r) * NT + t];
+                        cmac(acc[r], cplx<T>{(T)zz.x, (T)zz.y}, cplx<T>{(T)b.x, (T)b.y});
+                    }
+                    mbar_arrive(empty_bar(s));
+                }
+                F::inverse(acc, xp, s_tw, t, bar_id);
+                uint32_t *poly = s_acc + v * N;
+#pragma unroll
+                for (int r = 0; r < kR; r++) {
+                    const int j = t + NT * r;
+                    poly[j] += round_f64_mod32(acc[r].re);  // (c_j - i c_{j+M})
+                    poly[j + M] += round_f64_mod32(-acc[r].im);
+                }
+            }
+        }
+        team_sync(kAllBar, consumers);
+    }
+
+    uint32_t *dst = reinterpret_cast<uint32_t *>(args.acc_out) + (size_t)boot * KP1 * N;
+    for (int i = tid; i < KP1 * N; i += consumers) dst[i] = s_acc[i];
+}
+
 // ---- launch -------------------------------------------------------------------------------------
 
 template <typename T, int N, int L, bool SPLIT, int G, int D>
@@ -477,6 +716,16 @@ static cudaError_t launch_g(const BrArgs &a, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     const int grid = (a.boots + G - 1) / G;
     kern<<<grid, G * (N / 16) + 32, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename T, int N, int L, bool SPLIT, int D, int XB>
+static cudaError_t launch_wide(const BrArgs &a, cudaStream_t s) {
+    using Lay = WideLayout<T, N, 1, L, D, XB>;
+    auto kern = blind_rotate_wide_kernel<T, N, 1, L, SPLIT, D, XB>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::bytes);
+    if (e != cudaSuccess) return e;
+    kern<<<a.boots, 2 * L * (N / 16) + 32, Lay::bytes, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -503,11 +752,13 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_SPLIT_FP32, 3, 4, false, launch_g<float, 1024, 3, true, 3, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 2, 4, false, launch_g<float, 1024, 3, true, 2, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 3, true, 1, 4>},
+    {1024, 3, TFHEB_SPLIT_FP32, 1, 8, false, launch_wide<float, 1024, 3, true, 8, 2>},
     {1024, 3, TFHEB_FP64, 4, 6, true, launch_g<double, 1024, 3, false, 4, 6>},
     {1024, 3, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 3, false, 4, 4>},
     {1024, 3, TFHEB_FP64, 3, 4, true, launch_g<double, 1024, 3, false, 3, 4>},
     {1024, 3, TFHEB_FP64, 2, 4, true, launch_g<double, 1024, 3, false, 2, 4>},
     {1024, 3, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 3, false, 1, 4>},
+    {1024, 3, TFHEB_FP64, 1, 6, false, launch_wide<double, 1024, 3, false, 6, 1>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_g<float, 2048, 3, true, 2, 4>},
     {2048, 3, TFHEB_SPLIT_FP32, 3, 3, true, launch_g<float, 2048, 3, true, 3, 3>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 3, true, launch_g<float, 2048, 3, true, 2, 3>},
@@ -596,12 +847,15 @@ cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const Devi
             const int e = choice.small[need];
             if (e >= 0 && e < br_variant_count()) {
                 g = e;
-            } else if (e == -2) {
+            } else if (e == -2) {  // fewest bootstraps per CTA that fit; of equals, the later entry
+                int pick = -1;
                 for (int i = 0; i < br_variant_count(); i++) {
                     const BrVariant &v = kBrVariants[i];
-                    if (v.N == p.N && v.l == p.l && v.precision == precision && v.G >= need && v.G < kBrVariants[g].G)
-                        g = i;
+                    if (v.N == p.N && v.l == p.l && v.precision == precision && v.G >= need &&
+                        v.G < kBrVariants[g].G && (pick < 0 || v.G <= kBrVariants[pick].G))
+                        pick = i;
                 }
+                if (pick >= 0) g = pick;
             }
         }
     }
