@@ -268,8 +268,12 @@ def test_80bit_params_all_gates_and_a_4096_batch(keys80, precision):
         bits, _ = sk.decrypt(ck.gate(code, ca, cb, cc if code == 10 else None, precision=precision))
         assert (bits == TRUTH[code](a, b, c)).all(), f"gate {tb.api.GATE_NAMES[code]}"
     x, y = rng.integers(0, 2, (2, 4096))
-    bits, ph = sk.decrypt(ck.gate(tb.api.NAND, sk.encrypt(x, seed=4), sk.encrypt(y, seed=5), precision=precision))
+    ex, ey = sk.encrypt(x, seed=4), sk.encrypt(y, seed=5)
+    out = ck.gate(tb.api.NAND, ex, ey, precision=precision)
+    bits, ph = sk.decrypt(out)
     assert (bits == 1 - (x & y)).all()
+    # 64 gates run one bootstrap per CTA (the digit-parallel kernel), 4096 run packed: same bits
+    assert (ck.gate(tb.api.NAND, ex[:64], ey[:64], precision=precision) == out[:64]).all()
     # outputs sit at +-1/8 = +-2^29 Torus32 units; a decryption error needs |noise| > 2^29.  With
     # 10-bit digits the split form's low limb carries S = 27 bits, so its FP32 error adds to the
     # noise; both forms keep the rms far below the margin.

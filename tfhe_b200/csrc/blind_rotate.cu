@@ -770,8 +770,10 @@ static const BrVariant kBrVariants[] = {
     // the 80-bit parameter set (n = 500, l = 2, Bgbit = 10; tfhe_gate_bootstrapping.cpp:23-48)
     {1024, 2, TFHEB_SPLIT_FP32, 7, 4, true, launch_g<float, 1024, 2, true, 7, 4>},
     {1024, 2, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 2, true, 1, 4>},
+    {1024, 2, TFHEB_SPLIT_FP32, 1, 8, false, launch_wide<float, 1024, 2, true, 8, 2>},
     {1024, 2, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 2, false, 4, 4>},
     {1024, 2, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 2, false, 1, 4>},
+    {1024, 2, TFHEB_FP64, 1, 6, false, launch_wide<double, 1024, 2, false, 6, 2>},
 };
 
 int br_variants(int N, int l, int precision, int *G, int *D, int cap) {
