@@ -203,6 +203,28 @@ def test_cmux_step_split_fp32_error_bound(oracle, request, ring):
     assert rms < scale * 2**14
 
 
+@pytest.mark.parametrize("precision", [tb.FP64, tb.SPLIT_FP32])
+def test_cmux_step_packed_and_digit_parallel_kernels(oracle, default_keys, precision):
+    # 1040 accumulators (more than one wave at 7 per CTA) run on the packed kernel; 6 of them again
+    # alone run on the digit-parallel kernel: the same bits, and samples of the large batch within
+    # the single-step bounds of the exact oracle
+    p, sk, ck, bsk, ksk = default_keys
+    rng = np.random.default_rng(11 + precision)
+    count = 1040
+    acc = rng.integers(-2**31, 2**31, (count, p.k + 1, p.N), dtype=np.int64).astype(np.int32)
+    a = rng.integers(1, 2 * p.N, count).astype(np.int32)
+    d_acc = dev(acc)
+    ck.blind_rotate_device(dev(a.reshape(count, 1)), d_acc, count, 1, precision=precision)
+    big = host(d_acc)
+    d_small = dev(acc[:6])
+    ck.blind_rotate_device(dev(a[:6].reshape(6, 1)), d_small, 6, 1, precision=precision)
+    assert (host(d_small) == big[:6]).all()
+    for gi in (0, 517, count - 1):
+        want = oracle.cmux_step(pdict(p), bsk[0], a[gi], acc[gi].reshape(-1))
+        err = torus_diff(big[gi].reshape(-1), want)
+        assert np.abs(err).max() <= (1 if precision == tb.FP64 else 2**17)
+
+
 def test_blind_rotate_many_steps_fp64_matches_oracle(oracle, default_keys):
     # 40 consecutive CMUX steps from a random accumulator: FP64 products round to the exact value,
     # so the GPU accumulator equals the oracle's almost everywhere (a rare +-1 can flip a digit).
