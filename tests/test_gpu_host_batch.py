@@ -122,11 +122,21 @@ def test_small_batches_match_large_batches_bit_for_bit(keys, precision):
         assert (got == 1 - (x & y)).all()
 
 
+@pytest.fixture(scope="module")
+def large_keys():
+    p = tb.large_params()
+    sk, ck = tb.keygen(p, seed=2048)
+    ck.to_device(0)
+    return p, sk, ck
+
+
+@pytest.mark.parametrize("ring", ["default", "large"])
 @pytest.mark.parametrize("precision", [tb.FP64, tb.SPLIT_FP32])
-def test_every_tuned_variant_gives_the_same_bits(keys, precision):
+def test_every_tuned_variant_gives_the_same_bits(request, ring, precision):
     # 1036 gates need 7 bootstraps per CTA for one wave, no fewer than any candidate packs, so no
-    # small-batch variant stands in: packing, ring depth and paired transforms must not change a bit
-    p, sk, ck = keys
+    # small-batch variant stands in: packing, ring depth, paired transforms and who streams the key
+    # must not change a bit
+    p, sk, ck = request.getfixturevalue("keys" if ring == "default" else "large_keys")
     rng = np.random.default_rng(120 + precision)
     x, y = rng.integers(0, 2, 1036), rng.integers(0, 2, 1036)
     a, b = sk.encrypt(x, seed=121), sk.encrypt(y, seed=122)

@@ -72,7 +72,7 @@ struct DigitConv<double> {
 
 // ---- shared-memory layout ---------------------------------------------------------------------
 
-template <typename T, int N, int K, int G, int D>
+template <typename T, int N, int K, int G, int D, bool PW = true>
 struct BrLayout {
     static constexpr int M = N / 2, NT = M / kR, KP1 = K + 1;
     static constexpr uint32_t chunk = (uint32_t)KP1 * M * 16;  // one key row (step, p): all v, all slots
@@ -93,8 +93,9 @@ struct BrLayout {
     // measured faster than the scratch (36.15 ms per 4096 split bootstraps at G = 7, D = 6 without it,
     // 36.6 ms at D = 4 with it), and a lone team with 255 registers runs slower with it.
     static constexpr size_t kMaxSmem = 227 * 1024;
+    static constexpr int threads = G * (N / 16) + (PW ? 32 : 0);
     static constexpr bool rot_in_smem =
-        G * (N / 16) + 32 > 256 && teams + G * (team_acc + team_buf + 4 * (size_t)N) <= kMaxSmem;
+        threads > 256 && teams + G * (team_acc + team_buf + 4 * (size_t)N) <= kMaxSmem;
     static constexpr size_t team_rot = rot_in_smem ? 4 * (size_t)N : 0;
     __host__ __device__ static size_t team_bytes(int) { return team_acc + team_buf + team_rot; }
     __host__ __device__ static size_t bytes(int nsteps) { return teams + G * team_bytes(nsteps); }
@@ -127,9 +128,13 @@ __device__ __forceinline__ uint32_t rot_minus_one(const uint32_t *poly, int j, i
     return ((poly[e & (N - 1)] ^ neg) - neg) - poly[j];
 }
 
-template <typename T, int N, int K, int L, bool SPLIT, int G, int D>
-__global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const BrArgs args) {
-    using Lay = BrLayout<T, N, K, G, D>;
+// PW: a key-streaming warp issues the row copies.  Without it (G teams only), thread 0 issues them:
+// the first D at the start, then each row as soon as every team has released its slot, tested after
+// each of its own rows and waited for only when thread 0 needs a row not yet issued.  That frees the
+// producer warp's registers: 4 FP64 teams are 256 threads, which may use 255 registers each.
+template <typename T, int N, int K, int L, bool SPLIT, int G, int D, bool PW = true>
+__global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_kernel(const BrArgs args) {
+    using Lay = BrLayout<T, N, K, G, D, PW>;
     constexpr int M = N / 2, NT = M / kR, KP1 = K + 1, KPL = KP1 * L;
     using F = TeamFft<T, M, kR>;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -160,6 +165,16 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
     __syncthreads();
 
     const int total_chunks = args.nsteps * KPL;
+    // row c into its ring slot (the slot's previous row released by every team)
+    auto issue_row = [&](int c) {
+        const int s = c % D;
+        mbar_arrive_expect_tx(full_bar(s), Lay::chunk);
+        bulk_copy_g2s(ring + (uint32_t)s * Lay::chunk, args.bsk + (size_t)c * Lay::chunk, Lay::chunk, full_bar(s));
+    };
+    int issued = 0;        // !PW: rows issued by thread 0
+    bool issuing = !PW && tid == 0 && !args.stall_producer;
+    if (issuing)
+        for (; issued < min(D, total_chunks); issued++) issue_row(issued);
 
     // ---------------- producer warp: stream the key rows ----------------
     if (tid >= consumers) {
@@ -259,12 +274,23 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
         // same order as one at a time; the inverse that follows must be a pair (it begins with a
         // barrier).  One wave of 148 bootstraps at G = 1: 3.07 against 3.36 ms; at G = 3, 51.7 against
         // 53.6 ms per 4096.  The split form ran slower paired (3.97 against 3.20 ms at G = 1).
-        constexpr bool kPairInverse = G * NT + 32 <= 384;
+        constexpr bool kPairInverse = Lay::threads <= 384;
         constexpr bool kPairForward =
-            !SPLIT && G * NT + 32 <= 256 && !Lay::rot_in_smem && KPL % 2 == 0 && kPairInverse && KP1 == 2;
+            !SPLIT && Lay::threads <= 256 && !Lay::rot_in_smem && KPL % 2 == 0 && kPairInverse && KP1 == 2;
         // one digit's spectrum times key row c into the accumulators; frees the row's ring slot
         auto accumulate = [&](const cplx<T> *z) {
             const int s = c % D;
+            if constexpr (!PW) {
+                // thread 0 issues every row before anyone waits for it
+                while (issuing && issued <= c && issued < total_chunks) {
+                    if (!wait_bounded(empty_bar(issued % D), ((issued / D) - 1) & 1, abort_flag, args.timeout_ns,
+                                      args.err)) {
+                        issuing = false;
+                        break;
+                    }
+                    issue_row(issued++);
+                }
+            }
             wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns, args.err);
             const unsigned char *stage = smem + Lay::ring + (size_t)s * Lay::chunk;
             if constexpr (SPLIT) {
@@ -292,6 +318,10 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
                     }
             }
             mbar_arrive(empty_bar(s));
+            if constexpr (!PW) {
+                while (issuing && issued < total_chunks && mbar_test_wait(empty_bar(issued % D), ((issued / D) - 1) & 1))
+                    issue_row(issued++);
+            }
             c++;
         };
         // digit q of the words x[r] (a_j) and x[kR + r] (a_{j+M}), j = t + NT * r
@@ -464,6 +494,14 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_kernel(const
 
     uint32_t *dst = reinterpret_cast<uint32_t *>(args.acc_out) + (size_t)boot * KP1 * N;
     for (int i = t; i < KP1 * N; i += NT) dst[i] = s_acc[i];
+    if constexpr (!PW) {
+        // after an abort, drain the copies still in flight before the CTA may exit (bounded waits)
+        if (tid == 0) {
+            volatile int32_t no_abort = 0;
+            for (int r = (issued > D ? issued - D : 0); r < issued; r++)
+                wait_bounded(full_bar(r % D), (r / D) & 1, &no_abort, args.timeout_ns, args.err);
+        }
+    }
 }
 
 // ---- one bootstrap per CTA, digits in parallel ------------------------------------------------
@@ -707,15 +745,15 @@ __global__ void __launch_bounds__((K + 1) * L * (N / 16) + 32, 1) blind_rotate_w
 
 // ---- launch -------------------------------------------------------------------------------------
 
-template <typename T, int N, int L, bool SPLIT, int G, int D>
+template <typename T, int N, int L, bool SPLIT, int G, int D, bool PW = true>
 static cudaError_t launch_g(const BrArgs &a, cudaStream_t s) {
-    using Lay = BrLayout<T, N, 1, G, D>;
+    using Lay = BrLayout<T, N, 1, G, D, PW>;
     const size_t smem = Lay::bytes(a.nsteps);
-    auto kern = blind_rotate_kernel<T, N, 1, L, SPLIT, G, D>;
+    auto kern = blind_rotate_kernel<T, N, 1, L, SPLIT, G, D, PW>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = (a.boots + G - 1) / G;
-    kern<<<grid, G * (N / 16) + 32, smem, s>>>(a);
+    kern<<<grid, Lay::threads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -733,7 +771,8 @@ int blind_rotate_supported(const tfheb_params &p) {
     return br_variants(p.N, p.l, p.k == 1 ? TFHEB_FP64 : -1, nullptr, nullptr, 0) > 0;
 }
 
-// Compiled launch variants: (ring degree, precision, bootstraps per CTA G, key-ring depth D).
+// Compiled launch variants: (ring degree, precision, bootstraps per CTA G, key-ring depth D, and
+// whether a producer warp streams the key; without it, thread 0 does).
 // Every variant's shared memory stays within 227 KB.  Tuned variants are the autotuner's candidates:
 // the first of a (N, l, precision) triple is the default, and tfheb_autotune times all of them on the
 // device and keeps the fastest per key.  Small variants (few bootstraps per CTA) serve batches that
@@ -753,16 +792,19 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_SPLIT_FP32, 2, 4, false, launch_g<float, 1024, 3, true, 2, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 3, true, 1, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 1, 8, false, launch_wide<float, 1024, 3, true, 8, 2>},
+    {1024, 3, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 3, false, 4, 4, false>},
     {1024, 3, TFHEB_FP64, 4, 6, true, launch_g<double, 1024, 3, false, 4, 6>},
     {1024, 3, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 3, false, 4, 4>},
     {1024, 3, TFHEB_FP64, 3, 4, true, launch_g<double, 1024, 3, false, 3, 4>},
     {1024, 3, TFHEB_FP64, 2, 4, true, launch_g<double, 1024, 3, false, 2, 4>},
     {1024, 3, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 3, false, 1, 4>},
     {1024, 3, TFHEB_FP64, 1, 6, false, launch_wide<double, 1024, 3, false, 6, 1>},
+    {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_g<float, 2048, 3, true, 2, 4, false>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_g<float, 2048, 3, true, 2, 4>},
     {2048, 3, TFHEB_SPLIT_FP32, 3, 3, true, launch_g<float, 2048, 3, true, 3, 3>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 3, true, launch_g<float, 2048, 3, true, 2, 3>},
     {2048, 3, TFHEB_SPLIT_FP32, 1, 3, false, launch_g<float, 2048, 3, true, 1, 3>},
+    {2048, 3, TFHEB_FP64, 2, 3, true, launch_g<double, 2048, 3, false, 2, 3, false>},
     {2048, 3, TFHEB_FP64, 2, 3, true, launch_g<double, 2048, 3, false, 2, 3>},
     {2048, 3, TFHEB_FP64, 1, 4, true, launch_g<double, 2048, 3, false, 1, 4>},
     {512, 3, TFHEB_SPLIT_FP32, 8, 4, true, launch_g<float, 512, 3, true, 8, 4>},
@@ -771,6 +813,7 @@ static const BrVariant kBrVariants[] = {
     {1024, 2, TFHEB_SPLIT_FP32, 7, 4, true, launch_g<float, 1024, 2, true, 7, 4>},
     {1024, 2, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 2, true, 1, 4>},
     {1024, 2, TFHEB_SPLIT_FP32, 1, 8, false, launch_wide<float, 1024, 2, true, 8, 2>},
+    {1024, 2, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 2, false, 4, 4, false>},
     {1024, 2, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 2, false, 4, 4>},
     {1024, 2, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 2, false, 1, 4>},
     {1024, 2, TFHEB_FP64, 1, 6, false, launch_wide<double, 1024, 2, false, 6, 2>},
