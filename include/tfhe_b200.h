@@ -232,7 +232,8 @@ tfheb_status tfheb_measure_fma_peak(int32_t device, int32_t precision, double *t
 
 /* Blind-rotation launch variants an autotuner chooses from, for ring degree N, gadget length l = 3
  * (the 128-bit and N = 2048 sets) and a precision: bootstraps per CTA (teams_per_cta) and key-ring
- * depth; *count receives how many exist (arrays filled up to cap).  tfheb_cloud_key_br_variants
+ * depth; *count receives how many exist (arrays filled up to cap).  Two entries may share both
+ * numbers: one streams the key with a dedicated warp, the other from its first thread.  tfheb_cloud_key_br_variants
  * lists them for a key's own parameter set (the 80-bit set has l = 2).  tfheb_set_br_variant picks
  * one for a key; tfheb_autotune times them all on `boots` synthetic bootstraps, keeps the fastest
  * for the key, and writes each variant's time to ms[] (up to cap).  It then times, for each g below
