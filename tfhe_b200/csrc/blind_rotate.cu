@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_k
     // ---------------- producer warp: stream the key rows ----------------
     if (tid >= consumers) {
         if (tid == consumers) {
-            int issued = 0;
+            int sent = 0;
             if (!args.stall_producer) {
                 for (int c = 0; c < total_chunks; c++) {
                     const int s = c % D;
@@ -188,12 +188,12 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_k
                     mbar_arrive_expect_tx(full_bar(s), Lay::chunk);
                     bulk_copy_g2s(ring + (uint32_t)s * Lay::chunk, args.bsk + (size_t)c * Lay::chunk, Lay::chunk,
                                   full_bar(s));
-                    issued = c + 1;
+                    sent = c + 1;
                 }
             }
             // drain the copies still in flight before the CTA may exit (each wait bounded)
             volatile int32_t no_abort = 0;
-            for (int c = (issued > D ? issued - D : 0); c < issued; c++)
+            for (int c = (sent > D ? sent - D : 0); c < sent; c++)
                 wait_bounded(full_bar(c % D), (c / D) & 1, &no_abort, args.timeout_ns, args.err);
         }
         return;
