@@ -792,6 +792,7 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_SPLIT_FP32, 2, 4, false, launch_g<float, 1024, 3, true, 2, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 3, true, 1, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 1, 8, false, launch_wide<float, 1024, 3, true, 8, 2>},
+    {1024, 3, TFHEB_FP64, 4, 5, true, launch_g<double, 1024, 3, false, 4, 5, false>},
     {1024, 3, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 3, false, 4, 4, false>},
     {1024, 3, TFHEB_FP64, 4, 6, true, launch_g<double, 1024, 3, false, 4, 6>},
     {1024, 3, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 3, false, 4, 4>},
