@@ -140,3 +140,14 @@ def test_bench_script_parses_and_lists_its_workloads():
     assert res.returncode == 0, res.stderr
     for w in ("netlist", "mux2048", "errors", "keyswitch"):
         assert w in res.stdout
+
+
+def test_blind_rotation_defaults_listed_first():
+    # the first candidate of each parameter set is the default until tfheb_autotune measures
+    # otherwise: split G=7 D=6 and FP64 G=4 D=5 at N=1024 (l=3); G=2 at N=2048
+    want = {(1024, tb.SPLIT_FP32): (7, 6), (1024, tb.FP64): (4, 5),
+            (2048, tb.SPLIT_FP32): (2, 4), (2048, tb.FP64): (2, 3)}
+    for (N, prec), gd in want.items():
+        G, D = tb.api.br_variants(N, prec)
+        assert len(G) >= 2 and (int(G[0]), int(D[0])) == gd
+        assert (G >= 1).all() and (D >= 3).all()
