@@ -239,7 +239,8 @@ tfheb_status tfheb_measure_fma_peak(int32_t device, int32_t precision, double *t
  * for the key, and writes each variant's time to ms[] (up to cap).  It then times, for each g below
  * the winner's bootstraps per CTA, every compiled variant that fits a full wave of SMs x g bootstraps
  * and keeps the fastest for such one-wave batches (without autotuning, one-wave batches use the
- * variant with the fewest bootstraps per CTA that fits).  Results never depend on the variant.  No
+ * variant with the fewest bootstraps per CTA that fits; at one per CTA, the variant that spreads a
+ * bootstrap's gadget digits over one team each, N = 1024).  Results never depend on the variant.  No
  * reference counterpart (the reference has one CPU code path). */
 tfheb_status tfheb_br_variants(int32_t N, int32_t precision, int32_t *teams_per_cta, int32_t *ring_depth,
                                int32_t cap, int32_t *count);
