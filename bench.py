@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--error-gates", type=int, default=1_003_520,
+                    help="gates per form of the decryption-error count after the timed steps (0: skip)")
     ap.add_argument("--workload", choices=["nand", "netlist", "mux2048", "errors", "keyswitch", "dropin"],
                     default="nand",
                     help="nand: the headline line (4096 NAND batches); the others print their own line: "
@@ -234,6 +236,50 @@ def run_extra_workload(args):
                 runs.append(json.loads(res.stdout.strip().splitlines()[-1]))
         out.update({"form": "split-FP32", "api": "bootsNAND (include/tfhe.h), one gate per call", "runs": runs})
     print(json.dumps(out), flush=True)
+
+
+def count_errors(ck, sk, form, total, stream, sptr, seed=90):
+    """Decryption errors over `total` bootsNAND gates in batches of 4096 on fresh encryptions (new
+    bits, new seeds per batch), device buffers through tfheb_gate_batch_device.  Host encryption and
+    decryption of the next and previous batches run in a worker thread while the GPU evaluates the
+    current one (the library's host calls release the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+    import torch
+
+    import tfhe_b200 as tb
+    prec = tb.SPLIT_FP32 if form == "split" else tb.FP64
+    B, p = 4096, sk.params
+    batches = -(-total // B)
+    rng = np.random.default_rng(seed)
+    dout = torch.zeros((B, p.n + 1), dtype=torch.int32, device="cuda")
+
+    def make(i):
+        bits = rng.integers(0, 2, (2, B))
+        return bits, sk.encrypt(bits[0], seed=seed * 100003 + 2 * i + 1), sk.encrypt(bits[1], seed=seed * 100003 + 2 * i + 2)
+
+    def check(bits, out):
+        got, _ = sk.decrypt(out)
+        return int((got != 1 - (bits[0] & bits[1])).sum())
+
+    t0 = time.perf_counter()
+    errors, pending = 0, None
+    with ThreadPoolExecutor(max_workers=2) as pool:
+        nxt = pool.submit(make, 0)
+        for i in range(batches):
+            bits, ha, hb = nxt.result()
+            if i + 1 < batches:
+                nxt = pool.submit(make, i + 1)
+            da, db = torch.from_numpy(ha).cuda(), torch.from_numpy(hb).cuda()
+            ck.gate_device(tb.api.NAND, da, db, None, dout, B, precision=prec, stream=sptr)
+            out = dout.cpu().numpy()  # synchronises with the stream's work
+            if pending is not None:
+                errors += pending.result()
+            pending = pool.submit(check, bits, out)
+        errors += pending.result()
+    return {"gates": batches * B, "errors": errors, "batches": batches,
+            "wall_s": round(time.perf_counter() - t0, 2)}
 
 
 class ClockSampler:
@@ -470,15 +516,27 @@ def main():
     got, _ = sk.decrypt(po.numpy())
     e2e_errors = int((got != 1 - (bits[0] & bits[1])).sum())
 
+    # decryption-error count over >= 10^6 fresh gates per form, outside every timed region
+    errors_1e6 = None
+    if args.error_gates > 0:
+        errors_1e6 = {form: count_errors(ck, sk, form, args.error_gates, stream, sptr, seed=90 + rank)
+                      for form in (args.form, other)}
+
     if rank == 0:
         br_ms = main_r["kernel_ms"][1]
         flops = FLOPS_PER_GATE[args.form] * B
         achieved = flops / (br_ms / 1e3) / 1e12
         pk = peak["fp32" if args.form == "split" else "fp64"]
+        # DRAM traffic of the default blind-rotation variant per launch of this batch, from a one-kernel
+        # ncu capture (profiles/traffic.json names the variant and the command)
         traffic = None
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tpath):
-            traffic = json.load(open(tpath)).get(f"blind_rotate_{args.form}_bytes_per_launch")
+            traffic = json.load(open(tpath)).get(f"blind_rotate_{args.form}")
+        # nominal CUDA-core peak at the highest SM clock seen: SMs x lanes x 2 flops x clock
+        sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+        lanes = 128 if args.form == "split" else 64
+        nominal = sms * lanes * 2 * (clk.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": main_r["total_ms"] / args.steps, "higher_is_better": True,
@@ -497,7 +555,11 @@ def main():
             "roofline": {"bound": "fp32" if args.form == "split" else "fp64", "kernel": "blind_rotate_kernel",
                          "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
                          "peak_source": "measured FMA-chain probe on this GPU (tfheb_measure_fma_peak)",
-                         "traffic": traffic,
+                         "peak_nominal": nominal, "frac_nominal": achieved / nominal,
+                         "nominal_source": f"{sms} SMs x {lanes} lanes x 2 flops x max SM clock",
+                         "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                         "traffic_variant": traffic.get("variant") if traffic else None,
+                         "traffic_source": traffic.get("source") if traffic else None,
                          "algorithmic": f"{FLOPS_PER_GATE[args.form] / 1e6:.2f} MFLOP/gate x {B} gates per launch"},
             "peaks_measured": peak,
             "autotune": {k: [{"teams_per_cta": g, "ring_depth": d, "ms": m} for g, d, m in v] for k, v in tuning.items()},
@@ -506,6 +568,7 @@ def main():
                     "d2h_bytes_per_step": B * (p.n + 1) * 4, "errors": e2e_errors,
                     "api": "tfheb_gate_batch (host buffers, pinned)"},
             "gpu_launches": main_r["launches"],
+            "errors_1e6": errors_1e6,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds, B)

@@ -298,14 +298,16 @@ tfheb_status tfheb_netlist_multi_run(tfheb_netlist_multi *nl, int32_t precision,
 void tfheb_netlist_multi_free(tfheb_netlist_multi *nl);
 
 /* Allocation-free variant of tfheb_gate_batch_device, for callers that cannot call cudaMalloc
- * (while a CUDA graph is being captured, in real-time or signal-handling code that must not enter
- * the allocator, or under a framework that owns all device memory).  No counterpart in the
- * reference, which has no device memory at all.  All scratch comes from one fixed 8 MiB device array
- * in the library, so a call allocates and frees nothing; it fits 565 binary / 327 MUX gates at the
- * default parameters (301 / 176 at N=2048) and rejects larger counts with TFHEB_ERR_INVALID.  The
- * array is shared by all calls on a device: calls that overlap on the GPU race, so keep them on
- * one stream.  The first call on a device looks up the array's address; make it before any stream
- * capture.  The key must already be on the device (tfheb_cloud_key_to_device). */
+ * (real-time or signal-handling code that must not enter the allocator, or a process whose device
+ * memory belongs to a framework's pool).  No counterpart in the reference, which has no device
+ * memory at all.  All scratch comes from one fixed 8 MiB device array in the library, so a call
+ * allocates and frees nothing; it fits 565 binary / 327 MUX gates at the default parameters (301 /
+ * 176 at N=2048) and rejects larger counts with TFHEB_ERR_INVALID.  Buffers are checked like
+ * tfheb_gate_batch_device's.  The array is shared by all calls on a device: calls that overlap on
+ * the GPU race, so keep them on one stream.  The first call on a device looks up the array's
+ * address; make it before any stream capture.  That address belongs to the device's context, so do
+ * not call this again on a device after cudaDeviceReset.  The key must already be on the device
+ * (tfheb_cloud_key_to_device). */
 tfheb_status tfheb_gate_batch_device_noalloc(tfheb_cloud_key *ck, int32_t gate, int32_t precision, int32_t count,
                                              const int32_t *d_a, const int32_t *d_b, const int32_t *d_c,
                                              int32_t *d_out, void *stream);

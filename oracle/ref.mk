@@ -2,12 +2,15 @@
 # own source files, without its CMake build system, into oracle/_ref/.
 # The result is test infrastructure only: the parity checker and the timed CPU baseline.
 #
-#   make -f oracle/ref.mk REF=/root/reference            (run from the repository root)
+#   make -f oracle/ref.mk REF=<reference checkout>       (run from the repository root)
+#
+# REF defaults to $TFHE_REFERENCE_DIR, else /root/reference.
 #
 # Flags follow the reference's "optim" build type (src/CMakeLists.txt:28: -O2 -DNDEBUG
 # -funroll-loops), except that -march=native is replaced by -march=x86-64-v3 (AVX2+FMA, the
 # ISA the spqlios-fma assembly needs) so the library also runs on other x86 hosts.
-REF      ?= /root/reference
+TFHE_REFERENCE_DIR ?= /root/reference
+REF      ?= $(TFHE_REFERENCE_DIR)
 SRC      := $(REF)/src/libtfhe
 SPQ      := $(SRC)/fft_processors/spqlios
 OUT      := oracle/_ref

@@ -19,6 +19,7 @@
 #include <tgsw.h>
 #include <polynomials.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cstring>
@@ -207,21 +208,32 @@ void rs_bootstrap_woks(void *h, int32_t mu, int32_t count, const int32_t *in, in
     delete_LweSample(x);
 }
 
-// lweKeySwitch on raw inputs [count][k*N+1] -> [count][n+1]
-void rs_keyswitch(void *h, int32_t count, const int32_t *in, int32_t *out) {
+// lweKeySwitch on raw inputs [count][k*N+1] -> [count][n+1], with each result's current_variance
+// (the keyswitching key's sample variances summed over the non-zero digits,
+// lwe-keyswitch-functions.cpp:114-129) into var[count] when var is not null.  The samples are spread
+// over the host's threads; lweKeySwitch keeps no shared state.
+void rs_keyswitch(void *h, int32_t count, const int32_t *in, int32_t *out, double *var) {
     RsKeys *keys = static_cast<RsKeys *>(h);
     const int32_t n = io_params(keys)->n;
     const LweParams *ext = &acc_params(keys)->extracted_lweparams;
     const int32_t kN = ext->n;
-    LweSample *x = new_LweSample(ext);
-    LweSample *r = new_LweSample(io_params(keys));
-    for (int32_t g = 0; g < count; g++) {
-        load_lwe(x, in + int64_t(g) * (kN + 1), kN);
-        lweKeySwitch(r, keys->sk->cloud.bkFFT->ks, x);
-        store_lwe(out + int64_t(g) * (n + 1), r, n);
-    }
-    delete_LweSample(r);
-    delete_LweSample(x);
+    const int32_t threads = std::max(1, std::min<int32_t>(count, (int32_t)std::thread::hardware_concurrency()));
+    auto work = [&](int32_t t) {
+        LweSample *x = new_LweSample(ext);
+        LweSample *r = new_LweSample(io_params(keys));
+        for (int32_t g = t; g < count; g += threads) {
+            load_lwe(x, in + int64_t(g) * (kN + 1), kN);
+            lweKeySwitch(r, keys->sk->cloud.bkFFT->ks, x);
+            store_lwe(out + int64_t(g) * (n + 1), r, n);
+            if (var) var[g] = r->current_variance;
+        }
+        delete_LweSample(r);
+        delete_LweSample(x);
+    };
+    std::vector<std::thread> pool;
+    for (int32_t t = 1; t < threads; t++) pool.emplace_back(work, t);
+    work(0);
+    for (auto &th : pool) th.join();
 }
 
 // ---- building blocks (no keys needed) ---------------------------------------------------------

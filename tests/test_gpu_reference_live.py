@@ -44,11 +44,18 @@ def test_reference_keys_gates_decrypt_with_reference(ref_keys, precision):
     assert (keys.decrypt(ref_out)[0] == 1 - (a[:8] & b[:8])).all()
 
 
-def test_gpu_keyswitch_equals_reference_lweKeySwitch(ref_keys):
+# 32 samples run the tiled kernel; from 256 on, the default is the register-key kernel, the one the
+# 4096-gate batches use
+@pytest.mark.parametrize("count", [32, 256, 4096])
+def test_gpu_keyswitch_equals_reference_lweKeySwitch(ref_keys, count):
     keys, p, ck, _ = ref_keys
-    rng = np.random.default_rng(5)
-    x = rng.integers(-2**31, 2**31, (32, p.k * p.N + 1), dtype=np.int64).astype(np.int32)
-    out = torch.zeros((32, p.n + 1), dtype=torch.int32, device="cuda")
-    ck.keyswitch_device(torch.from_numpy(x).cuda(), out, 32)
+    rng = np.random.default_rng(5 + count)
+    x = rng.integers(-2**31, 2**31, (count, p.k * p.N + 1), dtype=np.int64).astype(np.int32)
+    x[0] = 0
+    x[-1] = -1
+    out = torch.zeros((count, p.n + 1), dtype=torch.int32, device="cuda")
+    ck.keyswitch_device(torch.from_numpy(x).cuda(), out, count)
     torch.cuda.synchronize()
-    assert (out.cpu().numpy() == keys.keyswitch(x)).all()
+    got = out.cpu().numpy()
+    want = keys.keyswitch(x)
+    assert (got == want).all(), f"{(got != want).any(axis=1).sum()} of {count} samples differ"

@@ -1,8 +1,8 @@
 """The allocation-free gate entry point (tfheb_gate_batch_device_noalloc) against the regular one.
 
-Callers that cannot allocate device memory -- code recording a CUDA graph, real-time or signal-
-handling paths that must not enter the allocator, processes whose device memory belongs to a
-framework's pool -- use the variant whose scratch lives in a fixed device array inside the library.
+Callers that cannot allocate device memory -- real-time or signal-handling paths that must not
+enter the allocator, processes whose device memory belongs to a framework's pool -- use the variant
+whose scratch lives in a fixed device array inside the library.
 It launches the same kernels, so on the same inputs its ciphertexts must equal the regular entry
 point's bit for bit (the kernels are deterministic); two calls in a row check that the shared
 array's leftover contents from the previous call do not leak into the next one.
@@ -65,3 +65,26 @@ def test_noalloc_rejects_batches_beyond_its_fixed_scratch(keys):
     st = noalloc(ck, tb.api.NAND, tb.FP64, count, a, a, None, out)
     assert st == 1  # TFHEB_ERR_INVALID
     assert b"scratch" in tb.api.lib().tfheb_last_error()
+
+
+def test_noalloc_checks_buffers_and_counts_like_the_regular_entry_point(keys):
+    p, sk, ck = keys
+    L = tb.api.lib()
+    # an empty batch needs no buffers
+    assert noalloc(ck, tb.api.NAND, tb.FP64, 0, None, None, None, None) == 0
+    # a host buffer is refused on the host, before any kernel could touch it
+    host = np.zeros((4, p.n + 1), np.int32)
+    d = torch.zeros((4, p.n + 1), dtype=torch.int32, device="cuda")
+    L.tfheb_gate_batch_device_noalloc.argtypes = [V, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, V, V, V, V, V]
+    st = L.tfheb_gate_batch_device_noalloc(ck.h, tb.api.NAND, tb.FP64, 4, V(host.ctypes.data), V(d.data_ptr()),
+                                           None, V(d.data_ptr()), None)
+    assert st == 1 and b"d_a" in L.tfheb_last_error()
+    # NOT is one negation kernel, counted like the regular entry point counts it
+    bits = np.array([0, 1, 1, 0])
+    a = torch.from_numpy(sk.encrypt(bits, seed=9)).cuda()
+    out = torch.zeros_like(a)
+    before = tb.kernel_launches()
+    assert noalloc(ck, tb.api.NOT, tb.FP64, 4, a, None, None, out) == 0
+    torch.cuda.synchronize()
+    assert tb.kernel_launches() - before == 1
+    assert (sk.decrypt(out.cpu().numpy())[0] == 1 - bits).all()

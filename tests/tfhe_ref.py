@@ -75,11 +75,12 @@ class RefKeys:
         self.lib.rs_bootstrap_woks(self.h, mu, len(x), _p(x), _p(out))
         return out
 
-    def keyswitch(self, x):
+    def keyswitch(self, x, with_variance=False):
         x = _i32(x)
         out = np.zeros((len(x), self.n + 1), np.int32)
-        self.lib.rs_keyswitch(self.h, len(x), _p(x), _p(out))
-        return out
+        var = np.zeros(len(x), np.float64) if with_variance else None
+        self.lib.rs_keyswitch(self.h, len(x), _p(x), _p(out), _p(var))
+        return (out, var) if with_variance else out
 
     def extern_mul(self, i, acc):
         acc = _i32(acc).copy()

@@ -1,11 +1,11 @@
 // noalloc.cu -- the batched gate pipeline for callers that cannot allocate device memory.
 //
-// Who needs it: code that runs where cudaMalloc is not available or not allowed -- inside a
-// captured CUDA graph being recorded, in a real-time or signal-handling context that must not take
-// the allocator's locks or block on it, or in a host process whose device memory is carved up by a
-// framework that forbids allocations outside its own pool.  tfheb_gate_batch_device grows per-key
-// scratch buffers with cudaMalloc on demand; this variant instead takes all of its scratch from one
-// file-scope device array, so a call allocates nothing.
+// Who needs it: code that runs where cudaMalloc is not available or not allowed -- a real-time or
+// signal-handling context that must not take the allocator's locks or block on it, or a host
+// process whose device memory is carved up by a framework that forbids allocations outside its own
+// pool.  tfheb_gate_batch_device grows per-key scratch buffers with cudaMalloc on demand; this
+// variant instead takes all of its scratch from one file-scope device array, so a call allocates
+// nothing.
 //
 // Scratch: g_noalloc_scratch, kNoAllocScratchBytes = 8 MiB, held by every GPU that loads the library
 // until the process exits.  One call needs, per gate (MUX: two bootstraps per gate),
@@ -15,7 +15,9 @@
 // with TFHEB_ERR_INVALID; split them into several calls.
 //
 // Set-up: the first call on a device looks up the array's device address (cudaGetSymbolAddress,
-// with that device current) and caches it; make that first call before any stream capture.
+// with that device current) and caches it; make that first call before any stream capture.  The
+// cached address belongs to the device's context: a process that calls cudaDeviceReset must not
+// call this entry point on that device afterwards.
 //
 // The array is shared by every call in the process on that device and keeps the previous call's
 // contents.  Nothing in it has to start at zero: the descriptors are rewritten by a kernel at the
@@ -78,14 +80,27 @@ using namespace tfheb;
 extern "C" tfheb_status tfheb_gate_batch_device_noalloc(tfheb_cloud_key *c, int32_t gate, int32_t precision,
                                                         int32_t count, const int32_t *d_a, const int32_t *d_b,
                                                         const int32_t *d_c, int32_t *d_out, void *stream) {
-    if (!c || count < 0 || gate < 0 || gate > TFHEB_COPY || !d_a || !d_out) return TFHEB_ERR_INVALID;
-    if (gate == TFHEB_MUX && (!d_b || !d_c)) return TFHEB_ERR_INVALID;
-    if (gate < TFHEB_MUX && !d_b) return TFHEB_ERR_INVALID;
+    if (!c || count < 0 || gate < 0 || gate > TFHEB_COPY) return TFHEB_ERR_INVALID;
+    if (count > 0 && (!d_a || !d_out || (gate == TFHEB_MUX && (!d_b || !d_c)) || (gate < TFHEB_MUX && !d_b)))
+        return TFHEB_ERR_INVALID;
+    // far above what the fixed array holds at any parameter set; keeps the size arithmetic in range
+    constexpr int32_t kMaxCount = 1 << 20;
+    if (count > kMaxCount) {
+        set_error("tfheb_gate_batch_device_noalloc: " + std::to_string(count) +
+                  " gates exceed the fixed scratch array by far; split the batch");
+        return TFHEB_ERR_INVALID;
+    }
     std::lock_guard<std::mutex> lock(c->mu);
     CloudKey &ck = c->ck;
     tfheb_status st = prepare_device(ck, precision);
     if (st != TFHEB_OK) return st;
     if (count == 0) return TFHEB_OK;
+    // a host pointer or another GPU's memory would fault inside the kernels instead of returning
+    // an error (cudaPointerGetAttributes allocates nothing)
+    const void *bufs[4] = {d_a, d_b, d_c, d_out};
+    const char *names[4] = {"d_a", "d_b", "d_c", "d_out"};
+    for (int i = 0; i < 4; i++)
+        if ((st = check_device_ptr(ck, bufs[i], names[i])) != TFHEB_OK) return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
     const tfheb_params &p = ck.p;
     const int n1 = p.n + 1;
@@ -97,16 +112,17 @@ extern "C" tfheb_status tfheb_gate_batch_device_noalloc(tfheb_cloud_key *c, int3
             set_error(std::string("tfheb_gate_batch_device_noalloc: ") + cudaGetErrorString(e));
             return TFHEB_ERR_CUDA;
         }
+        if (gate == TFHEB_NOT) g_kernel_launches += 1;
         return TFHEB_OK;
     }
-    const int boots = gate == TFHEB_MUX ? 2 * count : count;
-    const int bs = bara_stride_for(p);
-    const int kN1 = p.k * p.N + 1;
+    const size_t boots = gate == TFHEB_MUX ? 2 * (size_t)count : (size_t)count;
+    const size_t bs = (size_t)bara_stride_for(p);
+    const size_t kN1 = (size_t)p.k * p.N + 1;
     const size_t off_bd = 0;
-    const size_t off_gd = off_bd + align256(sizeof(BootDesc) * (size_t)boots);
+    const size_t off_gd = off_bd + align256(sizeof(BootDesc) * boots);
     const size_t off_bara = off_gd + align256(sizeof(GateDesc) * (size_t)count);
-    const size_t off_acc = off_bara + align256(4 * (size_t)boots * bs);
-    const size_t off_ksin = off_acc + align256(4 * (size_t)boots * (p.k + 1) * p.N);
+    const size_t off_acc = off_bara + align256(4 * boots * bs);
+    const size_t off_ksin = off_acc + align256(4 * boots * (p.k + 1) * (size_t)p.N);
     const size_t need = off_ksin + align256(4 * (size_t)count * kN1);
     if (need > kNoAllocScratchBytes) {
         set_error("tfheb_gate_batch_device_noalloc: " + std::to_string(count) + " gates need " +
@@ -132,13 +148,13 @@ extern "C" tfheb_status tfheb_gate_batch_device_noalloc(tfheb_cloud_key *c, int3
     fill_descs_kernel<<<(count + 255) / 256, 256, 0, s>>>(bd, gd, count, gate == TFHEB_MUX, cst, sa, sb,
                                                         modswitch_to_torus32(-1, 8), modswitch_to_torus32(1, 8));
     if ((e = cudaGetLastError()) == cudaSuccess)
-        e = launch_prologue(p, bd, boots, d_a, d_b, d_c, bara, bs, s);
+        e = launch_prologue(p, bd, (int)boots, d_a, d_b, d_c, bara, (int)bs, s);
     if (e == cudaSuccess)
-        e = launch_blind_rotate(p, precision, ck.dbsk[precision], bara, bs, boots, p.n, modswitch_to_torus32(1, 8),
-                                nullptr, acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns,
-                                ck.br[precision]);
-    if (e == cudaSuccess) e = launch_extract(p, gd, count, acc, ksin, kN1, s);
-    if (e == cudaSuccess) e = launch_keyswitch(ck, count, ksin, kN1, d_out, s);
+        e = launch_blind_rotate(p, precision, ck.dbsk[precision], bara, (int)bs, (int)boots, p.n,
+                                modswitch_to_torus32(1, 8), nullptr, acc, s, ck.d_err, ck.stall_producer,
+                                ck.wait_timeout_ns, ck.br[precision]);
+    if (e == cudaSuccess) e = launch_extract(p, gd, count, acc, ksin, (int)kN1, s);
+    if (e == cudaSuccess) e = launch_keyswitch(ck, count, ksin, (int)kN1, d_out, s);
     if (e != cudaSuccess) {
         set_error(std::string("tfheb_gate_batch_device_noalloc: ") + cudaGetErrorString(e));
         return TFHEB_ERR_CUDA;
