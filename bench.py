@@ -45,13 +45,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--error-gates", type=int, default=1_003_520,
                     help="gates per form of the decryption-error count after the timed steps (0: skip)")
-    ap.add_argument("--workload", choices=["nand", "netlist", "mux2048", "errors", "keyswitch", "dropin"],
+    ap.add_argument("--workload", choices=["nand", "netlist", "mux2048", "errors", "keyswitch", "dropin", "dft"],
                     default="nand",
                     help="nand: the headline line (4096 NAND batches); the others print their own line: "
                          "netlist = seeded 200-level random circuit through a CUDA graph, mux2048 = 1024 MUX "
                          "at N=2048, errors = decryption-error count over 10^6 split-FP32 NAND gates, "
                          "keyswitch = the three keyswitch kernels on --batch extracted samples, dropin = "
-                         "one bootsNAND per call through include/tfhe.h from 1, 16 and 64 threads")
+                         "one bootsNAND per call through include/tfhe.h from 1, 16 and 64 threads, dft = a "
+                         "radix-8 DFT stage on CUDA cores vs tensor cores (tfheb_measure_dft8)")
     ap.add_argument("--gates", type=int, default=1_000_000, help="gate count of --workload errors")
     ap.add_argument("--ring", type=int, choices=[1024, 2048], default=1024,
                     help="--workload errors: 1024 = NAND at the default parameters in the --form form "
@@ -235,6 +236,18 @@ def run_extra_workload(args):
                     raise RuntimeError(f"dropin_bench failed: {res.stdout}{res.stderr}")
                 runs.append(json.loads(res.stdout.strip().splitlines()[-1]))
         out.update({"form": "split-FP32", "api": "bootsNAND (include/tfhe.h), one gate per call", "runs": runs})
+    elif args.workload == "dft":
+        # one radix-8 stage of the blind rotation's FFT: CUDA-core codelet vs TF32x3 mma.sync
+        L = tb.api.lib()
+        L.tfheb_measure_dft8.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
+        names = {0: "cuda_core_dft8", 1: "mma_tf32x3_compute_only", 2: "mma_tf32x3_with_relayout"}
+        for method, name in names.items():
+            ns, err = ctypes.c_double(), ctypes.c_double()
+            st = L.tfheb_measure_dft8(0, method, ctypes.byref(ns), ctypes.byref(err))
+            if st != 0:
+                raise RuntimeError(L.tfheb_last_error().decode())
+            out[name] = {"ns_per_dft8_whole_gpu": ns.value, "max_rel_err_vs_fp64": err.value}
+        out["faster"] = min(names.values(), key=lambda k: out[k]["ns_per_dft8_whole_gpu"])
     print(json.dumps(out), flush=True)
 
 
@@ -562,7 +575,9 @@ def main():
                          "traffic_source": traffic.get("source") if traffic else None,
                          "algorithmic": f"{FLOPS_PER_GATE[args.form] / 1e6:.2f} MFLOP/gate x {B} gates per launch"},
             "peaks_measured": peak,
-            "autotune": {k: [{"teams_per_cta": g, "ring_depth": d, "ms": m} for g, d, m in v] for k, v in tuning.items()},
+            "autotune": tuning,
+            "plans": {"0": "radix-8 team FFT, one transform per thread",
+                      "1": "radix-8 team FFT, two transforms per thread on packed f32x2, digit spectra in TMEM"},
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * B * (p.n + 1) * 4,
                     "d2h_bytes_per_step": B * (p.n + 1) * 4, "errors": e2e_errors,

@@ -10,8 +10,13 @@
  *   TGswParams       tgsw.h:10-19
  *   TFheGateBootstrappingParameterSet / CloudKeySet / SecretKeySet
  *                    tfhe_gate_bootstrapping_structures.h:9-63
- * TGswKey, LweBootstrappingKey and LweBootstrappingKeyFFT are opaque here; the cloud keyset's
- * bkFFT points at the engine's device-resident key.
+ *   TorusPolynomial  polynomials.h:24-34        TLweSample  tlwe.h:47-51
+ *   TGswSample       tgsw.h:55-60               TGswSampleFFT tgsw.h:78-83
+ *   LweBootstrappingKey / LweBootstrappingKeyFFT  lwebootstrappingkey.h:10-16, 36-42
+ * TGswKey, LweKeySwitchKey and TLweSampleFFT are opaque here.  A cloud keyset's bk->bk is a view of
+ * the coefficient-domain key on the host (TGswSample rows whose polynomials point into the key's
+ * memory: read them, do not write them); its bkFFT->bkFFT array stands for the FFT-domain key, which
+ * lives on the GPU (each TLweSampleFFT is a handle of one key row).
  *
  * Every bootstrapped gate runs on the GPU (no CPU fallback).  The drop-in keeps the reference's
  * FP64 precision by default; tfhe_b200_set_precision selects the split-FP32 form.
@@ -68,8 +73,52 @@ typedef struct LweKey {
 } LweKey;
 
 typedef struct TGswKey TGswKey;
-typedef struct LweBootstrappingKey LweBootstrappingKey;
-typedef struct LweBootstrappingKeyFFT LweBootstrappingKeyFFT;
+typedef struct LweKeySwitchKey LweKeySwitchKey;
+typedef struct TLweSampleFFT TLweSampleFFT;
+
+typedef struct TorusPolynomial {
+    const int32_t N;
+    Torus32 *coefsT;
+} TorusPolynomial;
+
+typedef struct TLweSample {
+    TorusPolynomial *a;  /* k+1 polynomials: mask, then the body */
+    TorusPolynomial *b;  /* alias of a[k] */
+    double current_variance;
+    const int32_t k;
+} TLweSample;
+
+typedef struct TGswSample {
+    TLweSample *all_sample;   /* (k+1)*l rows */
+    TLweSample **bloc_sample; /* k+1 blocks of l rows */
+    const int32_t k;
+    const int32_t l;
+} TGswSample;
+
+typedef struct TGswSampleFFT {
+    TLweSampleFFT *all_samples; /* (k+1)*l row handles */
+    TLweSampleFFT **sample;     /* k+1 blocks of l handles */
+    const int32_t k;
+    const int32_t l;
+} TGswSampleFFT;
+
+typedef struct LweBootstrappingKey {
+    const LweParams *in_out_params;
+    const TGswParams *bk_params;
+    const TLweParams *accum_params;
+    const LweParams *extract_params;
+    TGswSample *bk;      /* n TGSW samples, coefficient domain (host view) */
+    LweKeySwitchKey *ks;
+} LweBootstrappingKey;
+
+typedef struct LweBootstrappingKeyFFT {
+    const LweParams *in_out_params;
+    const TGswParams *bk_params;
+    const TLweParams *accum_params;
+    const LweParams *extract_params;
+    const TGswSampleFFT *bkFFT; /* n TGSW samples, FFT domain (on the GPU) */
+    const LweKeySwitchKey *ks;
+} LweBootstrappingKeyFFT;
 
 typedef struct TFheGateBootstrappingParameterSet {
     const int32_t ks_t;
@@ -157,6 +206,55 @@ TFHE_B200_EXPORT void bootsNAND_batch(LweSample *results, const LweSample *a, co
                                       const TFheGateBootstrappingCloudKeySet *bk);
 TFHE_B200_EXPORT void bootsMUX_batch(LweSample *results, const LweSample *a, const LweSample *b, const LweSample *c,
                                      int32_t count, const TFheGateBootstrappingCloudKeySet *bk);
+
+/* ---- tfhe.h:36-43, tgsw_functions.h:40-46, lwe-functions.h:79: blind rotation, external product
+ * and keyswitch on single samples, on the GPU.
+ *   tfhe_blindRotate_FFT(accum, bk, bara, n, params): accum *= X^{sum bara_i s_i} over the n TGSW
+ *     samples bk[0..n-1]; bk must point into a keyset's bkFFT->bkFFT array (any offset).
+ *   tfhe_blindRotateAndExtract_FFT: the same from the test vector (0, X^{2N-barb} v), then the sample
+ *     extraction at index 0 into result (dimension kN).
+ *   tfhe_blindRotate / tfhe_blindRotateAndExtract: the same on coefficient-domain TGSW samples: a
+ *     keyset's bk->bk rows run on that key's device key; other TGSW samples are moved to the GPU and
+ *     transformed on every call (each call then allocates device memory).
+ *   tGswExternProduct(result, a, b, params): result = a (x) b; tGswExternMulToTLwe(accum, sample,
+ *     params): accum = sample (x) accum.
+ *   lweKeySwitch(result, ks, sample): ks must be a keyset's bk->ks or bkFFT->ks.
+ * The products use the FP64 FFT by default (split-FP32 after tfhe_b200_set_precision(1)); the
+ * reference's coefficient-domain functions compute them exactly, so their results may differ from
+ * it by a unit in rare coefficients.  Variances follow the reference's bookkeeping: the rotations
+ * keep accum's, tGswExternProduct and tGswExternMulToTLwe add ||digits||^2 times each TGSW row's
+ * variance (plus b's), lweKeySwitch and every keyswitched bootstrap sum the keyswitching-key rows'
+ * variances over the non-zero digits, and tfhe_bootstrap_woKS(_FFT) and the extractions leave the
+ * result's variance as it was. */
+TFHE_B200_EXPORT void tfhe_blindRotate_FFT(TLweSample *accum, const TGswSampleFFT *bk, const int32_t *bara,
+                                           const int32_t n, const TGswParams *bk_params);
+TFHE_B200_EXPORT void tfhe_blindRotateAndExtract_FFT(LweSample *result, const TorusPolynomial *v,
+                                                     const TGswSampleFFT *bk, const int32_t barb,
+                                                     const int32_t *bara, const int32_t n,
+                                                     const TGswParams *bk_params);
+TFHE_B200_EXPORT void tfhe_blindRotate(TLweSample *accum, const TGswSample *bk, const int32_t *bara, const int32_t n,
+                                       const TGswParams *bk_params);
+TFHE_B200_EXPORT void tfhe_blindRotateAndExtract(LweSample *result, const TorusPolynomial *v, const TGswSample *bk,
+                                                 const int32_t barb, const int32_t *bara, const int32_t n,
+                                                 const TGswParams *bk_params);
+TFHE_B200_EXPORT void tGswExternProduct(TLweSample *result, const TGswSample *a, const TLweSample *b,
+                                        const TGswParams *params);
+TFHE_B200_EXPORT void tGswExternMulToTLwe(TLweSample *accum, const TGswSample *sample, const TGswParams *params);
+TFHE_B200_EXPORT void lweKeySwitch(LweSample *result, const LweKeySwitchKey *ks, const LweSample *sample);
+
+/* ---- polynomials.h:97-103, tlwe.h:222-235, lwesamples.h:70-83: allocation of the samples above --- */
+TFHE_B200_EXPORT TorusPolynomial *new_TorusPolynomial(const int32_t N);
+TFHE_B200_EXPORT TorusPolynomial *new_TorusPolynomial_array(int32_t nbelts, const int32_t N);
+TFHE_B200_EXPORT void delete_TorusPolynomial(TorusPolynomial *obj);
+TFHE_B200_EXPORT void delete_TorusPolynomial_array(int32_t nbelts, TorusPolynomial *obj);
+TFHE_B200_EXPORT TLweSample *new_TLweSample(const TLweParams *params);
+TFHE_B200_EXPORT TLweSample *new_TLweSample_array(int32_t nbelts, const TLweParams *params);
+TFHE_B200_EXPORT void delete_TLweSample(TLweSample *obj);
+TFHE_B200_EXPORT void delete_TLweSample_array(int32_t nbelts, TLweSample *obj);
+TFHE_B200_EXPORT LweSample *new_LweSample(const LweParams *params);
+TFHE_B200_EXPORT LweSample *new_LweSample_array(int32_t nbelts, const LweParams *params);
+TFHE_B200_EXPORT void delete_LweSample(LweSample *obj);
+TFHE_B200_EXPORT void delete_LweSample_array(int32_t nbelts, LweSample *obj);
 
 /* ---- tfhe.h:38-39: coefficient-domain bootstrap (same GPU path as the _FFT forms) ------------ */
 TFHE_B200_EXPORT void tfhe_bootstrap(LweSample *result, const LweBootstrappingKey *bk, Torus32 mu, const LweSample *x);

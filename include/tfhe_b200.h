@@ -80,7 +80,9 @@ tfheb_status tfheb_keygen(const tfheb_params *p, uint64_t seed, tfheb_secret_key
 
 /* Import keys generated elsewhere (e.g. by the reference library), raw layouts:
  *   bsk [n][(k+1)*l][k+1][N] coefficient-domain TGSW rows (tgsw.h:55-60 all_sample order)
- *   ksk [k*N][ks_t][2^ks_basebit][n+1] (lwekeyswitch.h:11-28 ks0_raw order)
+ *   ksk [k*N][ks_t][2^ks_basebit][n+1] (lwekeyswitch.h:11-28 ks0_raw order); may be NULL for a key
+ *       that only serves blind rotations and external products (keyswitches and gates then return
+ *       TFHEB_ERR_INVALID, and the key cannot be saved)
  *   lwe_key [n], tlwe_key [k][N]. */
 tfheb_status tfheb_cloud_key_import(const tfheb_params *p, const int32_t *bsk, const int32_t *ksk,
                                     tfheb_cloud_key **ck);
@@ -154,6 +156,14 @@ tfheb_status tfheb_cloud_key_fft_download(const tfheb_cloud_key *ck, int32_t pre
 tfheb_status tfheb_gate_batch(tfheb_cloud_key *ck, int32_t gate, int32_t precision, int32_t count,
                               const int32_t *a, const int32_t *b, const int32_t *c, int32_t *out);
 
+/* tfheb_gate_batch plus, per gate, the number of keyswitching-key rows its keyswitch subtracted
+ * (the non-zero digits of lweKeySwitchTranslate_fromArray, lwe-keyswitch-functions.cpp:114-129):
+ * the reference's result current_variance is the sum of that many key-sample variances.  NOT and
+ * COPY report -1 (no keyswitch: the input's variance carries over, lwe-functions.cpp:111-126). */
+tfheb_status tfheb_gate_batch_terms(tfheb_cloud_key *ck, int32_t gate, int32_t precision, int32_t count,
+                                    const int32_t *a, const int32_t *b, const int32_t *c, int32_t *out,
+                                    int32_t *terms);
+
 /* The same batch sharded across several keys, each moved to its own GPU with
  * tfheb_cloud_key_to_device (keys with the same key material; the same device twice is allowed).
  * Shard k is rows [count*k/nkeys, count*(k+1)/nkeys), evaluated with tfheb_gate_batch on key k in
@@ -205,6 +215,29 @@ tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *ck, int32_t precision, i
 tfheb_status tfheb_keyswitch_device(tfheb_cloud_key *ck, int32_t count, const int32_t *d_in, int32_t *d_out,
                                     void *stream);
 
+/* The remaining scalar blind-rotation entry points, batched on device buffers:
+ *   tfheb_blind_rotate_steps_device   -> tfhe_blindRotate_FFT (lwe-bootstrapping-functions-fft.cpp:88-112)
+ *       over the key's TGSW samples first_step .. first_step+nsteps-1: acc [count][k+1][N] in place,
+ *       bara [count][nsteps] (values taken mod 2N)
+ *   tfheb_blind_rotate_extract_device -> tfhe_blindRotateAndExtract_FFT (:127-156): acc = (0,
+ *       X^{2N-barb} v) from v [count][N] and barb [count], the same rotation, then the sample
+ *       extraction at index 0 (lwe.cpp:41-53) into out [count][k*N+1]
+ *   tfheb_extern_product_device       -> tGswExternProduct (tgsw-functions.cpp:416-431) with the key's
+ *       TGSW sample `step`: out = bk_step (x) in, in/out [count][k+1][N] (may be the same buffer)
+ *   tfheb_ks_terms_device             -> the digit count of lweKeySwitch (lwe-keyswitch-functions.cpp:
+ *       114-129): terms [count] = non-zero digits of each extracted sample in [count][k*N+1]
+ * Asynchronous on `stream` (NULL: the key's stream), like the device calls above. */
+tfheb_status tfheb_blind_rotate_steps_device(tfheb_cloud_key *ck, int32_t precision, int32_t count, int32_t first_step,
+                                             int32_t nsteps, const int32_t *d_bara, int32_t *d_acc, void *stream);
+tfheb_status tfheb_blind_rotate_extract_device(tfheb_cloud_key *ck, int32_t precision, int32_t count,
+                                               int32_t first_step, int32_t nsteps, const int32_t *d_v,
+                                               const int32_t *d_barb, const int32_t *d_bara, int32_t *d_out,
+                                               void *stream);
+tfheb_status tfheb_extern_product_device(tfheb_cloud_key *ck, int32_t precision, int32_t count, int32_t step,
+                                         const int32_t *d_in, int32_t *d_out, void *stream);
+tfheb_status tfheb_ks_terms_device(tfheb_cloud_key *ck, int32_t count, const int32_t *d_in, int32_t *d_terms,
+                                   void *stream);
+
 /* Synchronise the key's stream and report any pending device error (TFHEB_ERR_TIMEOUT when a
  * bounded device-side wait of a kernel ran out). */
 tfheb_status tfheb_synchronize(tfheb_cloud_key *ck);
@@ -230,6 +263,15 @@ tfheb_status tfheb_profile_read(tfheb_cloud_key *ck, double *ms, int64_t *launch
  * measured by a dependent-chain probe kernel: the CUDA-core roofline denominator. */
 tfheb_status tfheb_measure_fma_peak(int32_t device, int32_t precision, double *tflops);
 
+/* Tensor cores or CUDA cores for a radix-8 stage of the FFT: applies 8-point complex DFTs to
+ * register-resident data over the whole GPU and reports the device time per DFT and the largest
+ * error relative to the column norm against FP64 DFTs.  method 0 = the FFT's dft8 codelet on the
+ * CUDA cores; 1 = the DFT as a 16x16 real matrix product with mma.sync m16n8k8 TF32 in three
+ * passes (FP32-level accuracy), operands kept in their fragment layouts (compute only); 2 = as 1,
+ * plus the warp shuffles that move each result into the next stage's operand layout.  No reference
+ * counterpart (the reference's FFT is AVX code on the CPU, spqlios-fft-fma.s). */
+tfheb_status tfheb_measure_dft8(int32_t device, int32_t method, double *ns_per_dft, double *max_rel_err);
+
 /* Blind-rotation launch variants an autotuner chooses from, for ring degree N, gadget length l = 3
  * (the 128-bit and N = 2048 sets) and a precision: bootstraps per CTA (teams_per_cta) and key-ring
  * depth; *count receives how many exist (arrays filled up to cap).  Two entries may share both
@@ -246,6 +288,12 @@ tfheb_status tfheb_br_variants(int32_t N, int32_t precision, int32_t *teams_per_
                                int32_t cap, int32_t *count);
 tfheb_status tfheb_cloud_key_br_variants(const tfheb_cloud_key *ck, int32_t precision, int32_t *teams_per_cta,
                                          int32_t *ring_depth, int32_t cap, int32_t *count);
+/* FFT plan of each variant of tfheb_cloud_key_br_variants, same order: 0 = the radix-8 team FFT with
+ * one transform per thread; 1 = the same transform, two per thread on packed f32x2, with the digit
+ * spectra parked in tensor memory and the multiply-accumulate one output polynomial at a time
+ * (split-FP32; the same bits as plan 0).  The autotuner times both plans. */
+tfheb_status tfheb_cloud_key_br_plans(const tfheb_cloud_key *ck, int32_t precision, int32_t *plan, int32_t cap,
+                                      int32_t *count);
 tfheb_status tfheb_set_br_variant(tfheb_cloud_key *ck, int32_t precision, int32_t variant);
 tfheb_status tfheb_autotune(tfheb_cloud_key *ck, int32_t precision, int32_t boots, double *ms, int32_t cap);
 

@@ -18,6 +18,7 @@
 #include <tlwe.h>
 #include <tgsw.h>
 #include <polynomials.h>
+#include <tgsw_functions.h>
 
 #include <algorithm>
 #include <atomic>
@@ -341,6 +342,23 @@ double rs_bench_gates(void *h, int gate, int32_t threads, int32_t gates_per_thre
 }  // extern "C"
 
 extern "C" {
+// tGswExternProduct with the coefficient-domain bootstrapping-key sample i: out = bk_i (x) b, both
+// [(k+1)][N], with b's current_variance b_var; the result's current_variance into *var
+void rs_extern_product(void *h, int32_t i, const int32_t *b, double b_var, int32_t *out, double *var) {
+    RsKeys *keys = static_cast<RsKeys *>(h);
+    const TLweParams *tp = acc_params(keys);
+    const int32_t N = tp->N, k = tp->k;
+    TLweSample *x = new_TLweSample(tp);
+    TLweSample *r = new_TLweSample(tp);
+    for (int32_t u = 0; u <= k; u++) std::memcpy(x->a[u].coefsT, b + u * N, sizeof(int32_t) * N);
+    x->current_variance = b_var;
+    tGswExternProduct(r, keys->sk->cloud.bk->bk + i, x, bk_params(keys));
+    for (int32_t u = 0; u <= k; u++) std::memcpy(out + u * N, r->a[u].coefsT, sizeof(int32_t) * N);
+    *var = r->current_variance;
+    delete_TLweSample(r);
+    delete_TLweSample(x);
+}
+
 // tGswFFTExternMulToTLwe with bootstrapping-key row i: acc[(k+1)][N] <- bkFFT[i] (*) acc
 void rs_extern_mul(void *h, int32_t i, int32_t *acc) {
     RsKeys *keys = static_cast<RsKeys *>(h);

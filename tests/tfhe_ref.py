@@ -82,6 +82,14 @@ class RefKeys:
         self.lib.rs_keyswitch(self.h, len(x), _p(x), _p(out), _p(var))
         return (out, var) if with_variance else out
 
+    def extern_product(self, i, b, b_var):
+        """tGswExternProduct with the coefficient-domain key sample i: (result, its variance)."""
+        b = _i32(b)
+        out = np.zeros_like(b)
+        var = ctypes.c_double()
+        self.lib.rs_extern_product(self.h, i, _p(b), ctypes.c_double(b_var), _p(out), ctypes.byref(var))
+        return out, var.value
+
     def extern_mul(self, i, acc):
         acc = _i32(acc).copy()
         self.lib.rs_extern_mul(self.h, i, _p(acc))

@@ -74,6 +74,7 @@ def lib():
         L.tfheb_fft_slot_order.argtypes = [_I32, _V]
         L.tfheb_br_variants.argtypes = [_I32, _I32, _V, _V, _I32, _V]
         L.tfheb_cloud_key_br_variants.argtypes = [_V, _I32, _V, _V, _I32, _V]
+        L.tfheb_cloud_key_br_plans.argtypes = [_V, _I32, _V, _I32, _V]
         L.tfheb_set_br_variant.argtypes = [_V, _I32, _I32]
         L.tfheb_autotune.argtypes = [_V, _I32, _I32, _V, _I32]
         L.tfheb_set_keyswitch_kernel.argtypes = [_V, _I32]
@@ -261,13 +262,24 @@ class CloudKey:
                "tfheb_cloud_key_br_variants")
         return G[:cnt.value], D[:cnt.value]
 
+    def br_plans(self, precision):
+        """FFT plan of each candidate variant: 0 = one transform per thread, 1 = two transforms per
+        thread on packed f32x2 with the digit spectra in tensor memory."""
+        cnt = ctypes.c_int32()
+        P = np.zeros(16, np.int32)
+        _check(lib().tfheb_cloud_key_br_plans(self.h, precision, _p(P), 16, ctypes.byref(cnt)),
+               "tfheb_cloud_key_br_plans")
+        return P[:cnt.value]
+
     def autotune(self, precision, boots=4096):
         """Times every candidate blind-rotation variant (and the small-batch ones, for one-wave
-        batches); returns [(teams_per_cta, ring_depth, ms)] of the candidates."""
+        batches); returns [{teams_per_cta, ring_depth, plan, ms}] of the candidates."""
         G, D = self.br_variants(precision)
+        P = self.br_plans(precision)
         ms = np.zeros(len(G), np.float64)
         _check(lib().tfheb_autotune(self.h, precision, boots, _p(ms), len(G)), "tfheb_autotune")
-        return list(zip(G.tolist(), D.tolist(), ms.tolist()))
+        return [{"teams_per_cta": int(g), "ring_depth": int(d), "plan": int(pl), "ms": float(m)}
+                for g, d, pl, m in zip(G, D, P, ms)]
 
     def set_br_variant(self, precision, variant):
         _check(lib().tfheb_set_br_variant(self.h, precision, variant), "tfheb_set_br_variant")

@@ -28,47 +28,11 @@
 #include <stdint.h>
 
 #include "async_copy.cuh"
+#include "br_common.cuh"
 #include "fft.cuh"
 #include "internal.h"
 
 namespace tfheb {
-
-// ---- exact conversions without the conversion (XU) pipe ------------------------------------
-
-// small non-negative integer d (d < 2^22) -> float d - (bias - 1.5*2^23): the bits of 1.5*2^23 + d are
-// 0x4B400000 | d, so the digit mask and this OR fuse into one logic op
-__device__ __forceinline__ float biased_to_float(uint32_t d, float bias) {
-    return __int_as_float(0x4B400000u | d) - bias;
-}
-// round-to-nearest of a float with |v| < 2^44, reduced mod 2^32 (FMA/ALU ops only)
-__device__ __forceinline__ uint32_t round_f32_mod32(float v) {
-    const float magic = 12582912.0f;  // 1.5 * 2^23
-    const float m1 = fmaf(v, 0x1.0p-22f, magic);
-    const uint32_t th = (uint32_t)(__float_as_int(m1) - 0x4B400000);
-    const float r = fmaf(-(m1 - magic), 4194304.0f, v);  // exact: |r| <= 2^21
-    const uint32_t tl = (uint32_t)(__float_as_int(r + magic) - 0x4B400000);
-    return (th << 22) + tl;
-}
-// round-to-nearest of a double with |v| < 2^51, reduced mod 2^32
-__device__ __forceinline__ uint32_t round_f64_mod32(double v) {
-    return (uint32_t)__double2loint(v + 6755399441055744.0);  // 1.5 * 2^52
-}
-
-template <typename T>
-struct DigitConv;
-template <>
-struct DigitConv<float> {
-    // value d - halfBg of a raw digit d in [0, Bg)
-    __device__ __forceinline__ static float conv(uint32_t d, float bias) { return biased_to_float(d, bias); }
-    __host__ __device__ static constexpr float base() { return 12582912.0f; }
-};
-template <>
-struct DigitConv<double> {
-    __device__ __forceinline__ static double conv(uint32_t d, double bias) {
-        return __hiloint2double(0x43380000, (int)d) - bias;
-    }
-    __host__ __device__ static constexpr double base() { return 6755399441055744.0; }
-};
 
 // ---- shared-memory layout ---------------------------------------------------------------------
 
@@ -103,36 +67,16 @@ struct BrLayout {
     static_assert(teams + G * (team_acc + team_buf) <= kMaxSmem, "shared memory of the variant");
 };
 
-struct BrArgs {
-    const int32_t *bara;
-    int bara_stride;
-    const uint8_t *bsk;
-    const void *tables;
-    const int32_t *acc_in;
-    int32_t *acc_out;
-    int boots, nsteps;
-    int32_t mu;
-    int Bgbit;
-    int split_shift;
-    int32_t *err;
-    uint64_t timeout_ns;
-    int stall_producer;
-};
 
-// (X^a - 1) * acc, coefficient j (toruspolynomial-functions.cpp:117-136), 0 <= a < 2N, without
-// branches: e = (j - a) mod 2N selects coefficient e mod N, negated when e >= N (X^N = -1).
-template <int N>
-__device__ __forceinline__ uint32_t rot_minus_one(const uint32_t *poly, int j, int a) {
-    const int e = (j - a) & (2 * N - 1);
-    const uint32_t neg = 0u - (uint32_t)((e & N) != 0);
-    return ((poly[e & (N - 1)] ^ neg) - neg) - poly[j];
-}
 
 // PW: a key-streaming warp issues the row copies.  Without it (G teams only), thread 0 issues them:
 // the first D at the start, then each row as soon as every team has released its slot, tested after
 // each of its own rows and waited for only when thread 0 needs a row not yet issued.  That frees the
 // producer warp's registers: 4 FP64 teams are 256 threads, which may use 255 registers each.
-template <typename T, int N, int K, int L, bool SPLIT, int G, int D, bool PW = true>
+// EXT: the external product alone (tGswExternProduct, tgsw-functions.cpp:416-431): each step computes
+// acc = bk_step (x) acc, without the rotation (X^a - 1) and without adding the old accumulator; the
+// rotation amounts are not read.  Only a few one-bootstrap-per-CTA variants are compiled with it.
+template <typename T, int N, int K, int L, bool SPLIT, int G, int D, bool PW = true, bool EXT = false>
 __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_kernel(const BrArgs args) {
     using Lay = BrLayout<T, N, K, G, D, PW>;
     constexpr int M = N / 2, NT = M / kR, KP1 = K + 1, KPL = KP1 * L;
@@ -212,8 +156,8 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_k
     uint32_t *s_rot = reinterpret_cast<uint32_t *>(tb + Lay::team_acc + Lay::team_buf);
     const cplx<T> *s_tw = s_tab;
 
-    const int32_t *my_bara = args.bara + (size_t)boot * args.bara_stride;
-    if (args.acc_in) {
+    const int32_t *my_bara = EXT ? nullptr : args.bara + (size_t)boot * args.bara_stride;
+    if (EXT || args.acc_in) {
         const uint32_t *src = reinterpret_cast<const uint32_t *>(args.acc_in) + (size_t)boot * KP1 * N;
         for (int i = t; i < KP1 * N; i += NT) s_acc[i] = src[i];
     } else {
@@ -242,10 +186,15 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_k
     const T digit_bias = DigitConv<T>::base() + T(1 << (Bgbit - 1));
 
     int c = 0;  // key-row (chunk) counter, same sequence as the producer
-    int a_next = args.nsteps > 0 ? my_bara[0] : 0;  // rotation amounts, loaded one step ahead
+    int a_next = (!EXT && args.nsteps > 0) ? my_bara[0] : 0;  // rotation amounts, loaded one step ahead
+    // the new accumulator word: the old one plus the product, or (EXT) the product alone
+    auto put = [](uint32_t &dst, uint32_t v) {
+        if constexpr (EXT) dst = v;
+        else dst += v;
+    };
     for (int step = 0; step < args.nsteps; step++) {
         const int ai = a_next & (2 * N - 1);
-        if (step + 1 < args.nsteps) a_next = my_bara[step + 1];
+        if (!EXT && step + 1 < args.nsteps) a_next = my_bara[step + 1];
         // FP64: one accumulator spectrum per output polynomial.  Split: hi- and lo-limb spectra as
         // packed register pairs over the slots (2m, 2m+1).
         cplx<T> acc_hi[SPLIT ? 1 : KP1][kR];
@@ -343,8 +292,8 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_k
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
                     const int j = t + NT * r;
-                    xr[u][r] = rot_minus_one<N>(s_acc + u * N, j, ai) + offset;
-                    xr[u][kR + r] = rot_minus_one<N>(s_acc + u * N, j + M, ai) + offset;
+                    xr[u][r] = (EXT ? s_acc[u * N + j] : rot_minus_one<N>(s_acc + u * N, j, ai)) + offset;
+                    xr[u][kR + r] = (EXT ? s_acc[u * N + j + M] : rot_minus_one<N>(s_acc + u * N, j + M, ai)) + offset;
                 }
 #pragma unroll 1
             for (int d = 0; d < KPL; d += 2) {
@@ -381,8 +330,8 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_k
 #pragma unroll
                 for (int r = 0; r < kR; r++) {
                     const int j = t + NT * r;
-                    const uint32_t v0 = rot_minus_one<N>(poly, j, ai) + offset;
-                    const uint32_t v1 = rot_minus_one<N>(poly, j + M, ai) + offset;
+                    const uint32_t v0 = (EXT ? poly[j] : rot_minus_one<N>(poly, j, ai)) + offset;
+                    const uint32_t v1 = (EXT ? poly[j + M] : rot_minus_one<N>(poly, j + M, ai)) + offset;
                     if constexpr (Lay::rot_in_smem) {
                         s_rot[r * NT + t] = v0;
                         s_rot[(kR + r) * NT + t] = v1;
@@ -421,10 +370,10 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_k
 #pragma unroll
             for (int r = 0; r < kR; r++) {
                 const int j = t + NT * r;
-                s_acc[j] += round_f64_mod32(z0[r].re);  // (c_j - i c_{j+M})
-                s_acc[j + M] += round_f64_mod32(-z0[r].im);
-                s_acc[N + j] += round_f64_mod32(z1[r].re);
-                s_acc[N + j + M] += round_f64_mod32(-z1[r].im);
+                put(s_acc[j], round_f64_mod32(z0[r].re));  // (c_j - i c_{j+M})
+                put(s_acc[j + M], round_f64_mod32(-z0[r].im));
+                put(s_acc[N + j], round_f64_mod32(z1[r].re));
+                put(s_acc[N + j + M], round_f64_mod32(-z1[r].im));
             }
         }
 #pragma unroll
@@ -485,8 +434,8 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_k
 #pragma unroll
             for (int r = 0; r < kR; r++) {
                 const int j = t + NT * r;
-                poly[j] += c0[r];
-                poly[j + M] += c1[r];
+                put(poly[j], c0[r]);
+                put(poly[j + M], c1[r]);
             }
         }
         team_sync(bar_id, NT);
@@ -767,6 +716,18 @@ static cudaError_t launch_wide(const BrArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// External product only (EXT), one sample per CTA, thread 0 streaming the key rows.
+template <typename T, int N, int L, bool SPLIT, int D>
+static cudaError_t launch_ext(const BrArgs &a, cudaStream_t s) {
+    using Lay = BrLayout<T, N, 1, 1, D, false>;
+    const size_t smem = Lay::bytes(a.nsteps);
+    auto kern = blind_rotate_kernel<T, N, 1, L, SPLIT, 1, D, false, true>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<a.boots, Lay::threads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
 int blind_rotate_supported(const tfheb_params &p) {
     return br_variants(p.N, p.l, p.k == 1 ? TFHEB_FP64 : -1, nullptr, nullptr, 0) > 0;
 }
@@ -782,12 +743,18 @@ struct BrVariant {
     int N, l, precision, G, D;
     bool tuned;
     cudaError_t (*launch)(const BrArgs &, cudaStream_t);
+    int plan = 0;  // 0: one transform per thread; 1: two per thread, spectra in TMEM (blind_rotate_paired.cu)
 };
 static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_SPLIT_FP32, 7, 6, true, launch_g<float, 1024, 3, true, 7, 6>},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 4, true, launch_g<float, 1024, 3, true, 7, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 5, 4, true, launch_g<float, 1024, 3, true, 5, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 4, 4, true, launch_g<float, 1024, 3, true, 4, 4>},
+    // plan 1: D counts half rows (8 KB) here; single or double exchange buffers per team
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 8, true, launch_paired<1024, 3, 7, 8, 1>, 1},
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired<1024, 3, 7, 12, 1>, 1},
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 4, true, launch_paired<1024, 3, 7, 4, 2>, 1},
+    {1024, 3, TFHEB_SPLIT_FP32, 6, 6, true, launch_paired<1024, 3, 6, 6, 2>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 3, 4, false, launch_g<float, 1024, 3, true, 3, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 2, 4, false, launch_g<float, 1024, 3, true, 2, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 3, true, 1, 4>},
@@ -805,6 +772,9 @@ static const BrVariant kBrVariants[] = {
     {2048, 3, TFHEB_SPLIT_FP32, 3, 3, true, launch_g<float, 2048, 3, true, 3, 3>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 3, true, launch_g<float, 2048, 3, true, 2, 3>},
     {2048, 3, TFHEB_SPLIT_FP32, 1, 3, false, launch_g<float, 2048, 3, true, 1, 3>},
+    {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_paired<2048, 3, 2, 4, 2>, 1},
+    {2048, 3, TFHEB_SPLIT_FP32, 2, 6, true, launch_paired<2048, 3, 2, 6, 2>, 1},
+    {2048, 3, TFHEB_SPLIT_FP32, 3, 4, true, launch_paired<2048, 3, 3, 4, 1>, 1},
     {2048, 3, TFHEB_FP64, 2, 3, true, launch_g<double, 2048, 3, false, 2, 3, false>},
     {2048, 3, TFHEB_FP64, 2, 3, true, launch_g<double, 2048, 3, false, 2, 3>},
     {2048, 3, TFHEB_FP64, 1, 4, true, launch_g<double, 2048, 3, false, 1, 4>},
@@ -836,8 +806,8 @@ int br_variants(int N, int l, int precision, int *G, int *D, int cap) {
 static BrArgs br_args(const tfheb_params &p, const DeviceBsk &bsk, const int32_t *bara, int bara_stride, int boots,
                       int nsteps, int32_t mu, const int32_t *acc_in, int32_t *acc_out, int32_t *d_err,
                       int stall_producer, uint64_t timeout_ns) {
-    return BrArgs{bara, bara_stride, reinterpret_cast<const uint8_t *>(bsk.bsk), bsk.tables, acc_in, acc_out, boots,
-                  nsteps, mu, p.Bgbit, bsk.split_shift, d_err, timeout_ns, stall_producer};
+    return BrArgs{bara,       bara_stride, reinterpret_cast<const uint8_t *>(bsk.bsk), bsk.tables, bsk.tables2, acc_in,
+                  acc_out,    boots,       nsteps, mu, p.Bgbit, bsk.split_shift, d_err, timeout_ns, stall_producer};
 }
 
 int br_variant_count() { return (int)(sizeof(kBrVariants) / sizeof(kBrVariants[0])); }
@@ -850,6 +820,18 @@ void br_variant_info(int g, int *N, int *l, int *precision, int *G, int *D, int 
     if (G) *G = v.G;
     if (D) *D = v.D;
     if (tuned) *tuned = v.tuned;
+}
+
+int br_variant_plan(int g) { return kBrVariants[g].plan; }
+
+int br_variant_plans(int N, int l, int precision, int *plan, int cap) {
+    int n = 0;
+    for (const auto &v : kBrVariants)
+        if (v.tuned && v.N == N && v.l == l && v.precision == precision) {
+            if (plan && n < cap) plan[n] = v.plan;
+            n++;
+        }
+    return n;
 }
 
 int br_tuned_global(int N, int l, int precision, int tuned) {
@@ -907,6 +889,32 @@ cudaError_t launch_blind_rotate(const tfheb_params &p, int precision, const Devi
     }
     return launch_blind_rotate_exact(p, precision, bsk, bara, bara_stride, boots, nsteps, mu, acc_in, acc_out, s, d_err,
                                      stall_producer, timeout_ns, g);
+}
+
+struct ExtVariant {
+    int N, l, precision;
+    cudaError_t (*launch)(const BrArgs &, cudaStream_t);
+};
+static const ExtVariant kExtVariants[] = {
+    {1024, 3, TFHEB_FP64, launch_ext<double, 1024, 3, false, 3>},
+    {1024, 3, TFHEB_SPLIT_FP32, launch_ext<float, 1024, 3, true, 3>},
+    {1024, 2, TFHEB_FP64, launch_ext<double, 1024, 2, false, 3>},
+    {1024, 2, TFHEB_SPLIT_FP32, launch_ext<float, 1024, 2, true, 3>},
+    {2048, 3, TFHEB_FP64, launch_ext<double, 2048, 3, false, 3>},
+    {2048, 3, TFHEB_SPLIT_FP32, launch_ext<float, 2048, 3, true, 3>},
+    {512, 3, TFHEB_FP64, launch_ext<double, 512, 3, false, 3>},
+    {512, 3, TFHEB_SPLIT_FP32, launch_ext<float, 512, 3, true, 3>},
+};
+
+cudaError_t launch_extern_product(const tfheb_params &p, int precision, const DeviceBsk &bsk, int count,
+                                  const int32_t *in, int32_t *out, cudaStream_t s, int32_t *d_err,
+                                  uint64_t timeout_ns) {
+    if (count <= 0) return cudaSuccess;
+    if (!in || !out) return cudaErrorInvalidValue;
+    for (const auto &v : kExtVariants)
+        if (v.N == p.N && v.l == p.l && v.precision == precision)
+            return v.launch(br_args(p, bsk, nullptr, 0, count, 1, 0, in, out, d_err, 0, timeout_ns), s);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace tfheb

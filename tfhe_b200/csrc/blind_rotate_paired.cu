@@ -1,0 +1,342 @@
+// blind_rotate_paired.cu -- the split-FP32 blind rotation with two transforms per thread and the
+// digit spectra in tensor memory (tfhe_blindRotate_FFT, lwe-bootstrapping-functions-fft.cpp:88-112,
+// with the external product tGswFFTExternMulToTLwe, tgsw-fft-operations.cpp:89-114).
+//
+// The same work, in the same order per accumulator, as blind_rotate_kernel<float, ..., SPLIT>, so
+// both give the same bits.  The schedule differs:
+//   * The gadget digits of a step are transformed two at a time on packed f32x2 (TeamFft2: one
+//     packed instruction performs the same scalar operation on both transforms), and each output
+//     polynomial's two key limbs are inverted together: half the FP32 instructions of the
+//     transforms, and one 16-byte exchange access per point of two transforms.
+//   * The (k+1)l digit spectra of a step are parked in tensor memory (TMEM, 256 KB per SM, which the
+//     path otherwise leaves idle), one 32-lane row per thread.  The multiply-accumulate then runs one
+//     output polynomial at a time, so two limb accumulators (32 registers) are live instead of
+//     2(k+1) (64 registers at k = 1), and the 128 registers of 15 warps per SM hold the paired
+//     transforms without spilling.
+//   * The key ring holds half rows, one output polynomial's slots of one digit row (8 KB at N =
+//     1024), streamed in the order of the multiply-accumulate: per step, output 0 over the digits,
+//     then output 1.
+// Every mbarrier wait is bounded as in blind_rotate_kernel.  Warp 0 allocates the TMEM columns at
+// the start and frees them after every consumer thread has passed a final barrier, on every path
+// (a wait that runs out only makes the remaining waits return at once).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "async_copy.cuh"
+#include "br_common.cuh"
+#include "fft.cuh"
+#include "internal.h"
+
+namespace tfheb {
+
+namespace {
+
+// ---- tensor memory ----------------------------------------------------------------------------
+// A warp reads and writes the 32 TMEM lanes of its quadrant (warp % 4); address = lane << 16 | column.
+
+__device__ __forceinline__ void tmem_alloc(uint32_t smem_dst, uint32_t cols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_dst), "r"(cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_free(uint32_t taddr, uint32_t cols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before_sync() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 consecutive columns of this thread's lane
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+        "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]),
+        "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]),
+        "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// 16 consecutive columns of this thread's lane, waited for in the same statement so that no use of
+// the registers can be scheduled before the data has arrived
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr)
+        : "memory");
+}
+
+}  // namespace
+
+// ---- shared memory and TMEM budget ---------------------------------------------------------------
+
+template <int N, int L, int G, int D, int XB>
+struct PairLayout {
+    static constexpr int M = N / 2, NT = M / kR, KP1 = 2, KPL = KP1 * L;
+    static constexpr uint32_t half = (uint32_t)M * 16;  // one output's slots of one key row
+    static constexpr size_t bars = 0;                   // full[D], empty[D], abort flag, TMEM address
+    static constexpr size_t ring = (2 * D * 8 + 8 + 127) / 128 * 128;
+    static constexpr size_t tables = ring + (size_t)D * half;
+    static constexpr size_t tables_bytes = 16 * (size_t)tw_offset<M>(FftPlan<M>::NS);
+    static constexpr size_t teams = tables + tables_bytes;
+    static constexpr size_t team_acc = 4 * (size_t)KP1 * N;
+    static constexpr size_t team_xbuf = 16 * (size_t)Exch<double, M>::slots;
+    static constexpr size_t team_bytes = team_acc + XB * team_xbuf;
+    static constexpr size_t bytes = teams + G * team_bytes;
+    static constexpr int threads = G * NT + 32;
+    // TMEM: KPL spectra of 16 words per thread; warps of one lane quadrant take column slots in turn
+    static constexpr int warps = G * NT / 32;
+    static constexpr int cols_per_warp = KPL * 16;
+    static constexpr int cols_needed = (warps + 3) / 4 * cols_per_warp;
+    static constexpr int tmem_cols = cols_needed <= 32 ? 32 : cols_needed <= 64 ? 64 : cols_needed <= 128 ? 128
+                                   : cols_needed <= 256 ? 256 : 512;
+    static_assert(cols_needed <= 512, "TMEM columns of the variant");
+    static_assert(bytes <= 227 * 1024, "shared memory of the variant");
+    static_assert(NT % 32 == 0, "whole warps per team");
+    static_assert(half % 16 == 0, "bulk copies need 16-byte sizes");
+};
+
+template <int N, int L, int G, int D, int XB>
+__global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_paired_kernel(const BrArgs args) {
+    using Lay = PairLayout<N, L, G, D, XB>;
+    constexpr int M = N / 2, NT = M / kR, KP1 = 2, KPL = KP1 * L;
+    using F2 = TeamFft2<M>;
+    extern __shared__ __align__(128) unsigned char smem[];
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int consumers = G * NT;
+    const int active_teams = min(G, args.boots - (int)blockIdx.x * G);
+    const uint32_t bar0 = smem_addr(smem + Lay::bars);
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (D + s); };
+    volatile int32_t *abort_flag = reinterpret_cast<volatile int32_t *>(smem + Lay::bars + 16 * D);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + Lay::bars + 16 * D + 4);
+    const uint32_t ring = smem_addr(smem + Lay::ring);
+
+    if (tid == 0) {
+        for (int s = 0; s < D; s++) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), (uint32_t)(active_teams * NT));
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();  // the allocation is a warp-wide instruction: warp 0 converged after thread 0's branch
+    if (warp == 0) tmem_alloc(smem_addr(tmem_slot), Lay::tmem_cols);
+    {
+        const int4 *g_tab = reinterpret_cast<const int4 *>(args.tables2);
+        int4 *s_tab4 = reinterpret_cast<int4 *>(smem + Lay::tables);
+        for (int i = tid; i < (int)(Lay::tables_bytes / 16); i += blockDim.x) s_tab4[i] = g_tab[i];
+    }
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const uint32_t tmem_base = *tmem_slot;
+
+    // half rows in consumption order: per step, output v = 0 then 1, each over the digits d
+    const int total_chunks = args.nsteps * KP1 * KPL;
+
+    // ---------------- producer warp: stream the key half rows ----------------
+    if (tid >= consumers) {
+        if (tid == consumers) {
+            int sent = 0;
+            if (!args.stall_producer) {
+                for (int c = 0; c < total_chunks; c++) {
+                    const int s = c % D;
+                    if (c >= D && !wait_bounded(empty_bar(s), ((c / D) - 1) & 1, abort_flag, args.timeout_ns, args.err))
+                        break;
+                    const int step = c / (KP1 * KPL), rem = c - step * (KP1 * KPL);
+                    const int v = rem / KPL, d = rem - v * KPL;
+                    const size_t src = ((size_t)(step * KPL + d) * KP1 + v) * Lay::half;
+                    mbar_arrive_expect_tx(full_bar(s), Lay::half);
+                    bulk_copy_g2s(ring + (uint32_t)s * Lay::half, args.bsk + src, Lay::half, full_bar(s));
+                    sent = c + 1;
+                }
+            }
+            volatile int32_t no_abort = 0;
+            for (int c = (sent > D ? sent - D : 0); c < sent; c++)
+                wait_bounded(full_bar(c % D), (c / D) & 1, &no_abort, args.timeout_ns, args.err);
+        }
+        return;
+    }
+
+    // ---------------- consumer teams ----------------
+    const int team = tid / NT;
+    const int t = tid - team * NT;
+    if (team >= active_teams) return;  // no TMEM use, not counted in any barrier below
+    const int boot = blockIdx.x * G + team;
+    const int bar_id = 1 + team;
+    constexpr int kAllBar = 15;
+    static_assert(G < kAllBar, "named barrier ids");
+
+    unsigned char *tb = smem + Lay::teams + (size_t)team * Lay::team_bytes;
+    uint32_t *s_acc = reinterpret_cast<uint32_t *>(tb);
+    ExchPair xp{tb + Lay::team_acc, XB == 2 ? (uint32_t)Lay::team_xbuf : 0u, 0u};
+    const float4 *s_tw2 = reinterpret_cast<const float4 *>(smem + Lay::tables);
+    // this thread's TMEM row: lane quadrant of its warp, the warp's column slot within the quadrant
+    const uint32_t tmem_row = tmem_base + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((warp >> 2) * Lay::cols_per_warp);
+
+    const int32_t *my_bara = args.bara + (size_t)boot * args.bara_stride;
+    if (args.acc_in) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(args.acc_in) + (size_t)boot * KP1 * N;
+        for (int i = t; i < KP1 * N; i += NT) s_acc[i] = src[i];
+    } else {
+        // acc = (0, X^{2N-barb} * [mu,...,mu])  (lwe-bootstrapping-functions-fft.cpp:142-145)
+        const int e = 2 * N - my_bara[args.nsteps];
+        for (int i = t; i < N; i += NT) s_acc[i] = 0u;
+        for (int j = t; j < N; j += NT) {
+            int src = j - e;
+            uint32_t neg = 0;
+            while (src < 0) {
+                src += N;
+                neg ^= 1u;
+            }
+            s_acc[N + j] = neg ? 0u - (uint32_t)args.mu : (uint32_t)args.mu;
+        }
+    }
+    team_sync(bar_id, NT);
+
+    // gadget constants (tgsw.cpp:7-29)
+    const int Bgbit = args.Bgbit;
+    uint32_t offset = 0;
+#pragma unroll
+    for (int q = 0; q < L; q++) offset += 1u << (32 - (q + 1) * Bgbit);
+    offset *= 1u << (Bgbit - 1);
+    const uint32_t maskBg = (1u << Bgbit) - 1u;
+    const float digit_bias = 12582912.0f + float(1 << (Bgbit - 1));
+
+    int a_next = args.nsteps > 0 ? my_bara[0] : 0;  // rotation amounts, loaded one step ahead
+    for (int step = 0; step < args.nsteps; step++) {
+        const int ai = a_next & (2 * N - 1);
+        if (step + 1 < args.nsteps) a_next = my_bara[step + 1];
+
+        // 1. (X^a - 1) * poly + offset of both polynomials, words j = t + NT r and j + M
+        uint32_t xr[KP1][2 * kR];
+#pragma unroll
+        for (int u = 0; u < KP1; u++)
+#pragma unroll
+            for (int r = 0; r < kR; r++) {
+                const int j = t + NT * r;
+                xr[u][r] = rot_minus_one<N>(s_acc + u * N, j, ai) + offset;
+                xr[u][kR + r] = rot_minus_one<N>(s_acc + u * N, j + M, ai) + offset;
+            }
+        // 2. digits two at a time in chain order d = u*L + q, forward transforms, spectra to TMEM
+#pragma unroll
+        for (int d0 = 0; d0 < KPL; d0 += 2) {
+            const int u0 = d0 / L, q0 = d0 % L, u1 = (d0 + 1) / L, q1 = (d0 + 1) % L;
+            const int sh0 = 32 - (q0 + 1) * Bgbit, sh1 = 32 - (q1 + 1) * Bgbit;
+            cpair z[kR];
+#pragma unroll
+            for (int r = 0; r < kR; r++) {
+                // a_j - i a_{j+M} of each digit polynomial; the twist is folded into the FFT
+                const float a0 = biased_to_float((xr[u0][r] >> sh0) & maskBg, digit_bias);
+                const float a1 = biased_to_float((xr[u0][kR + r] >> sh0) & maskBg, digit_bias);
+                const float b0 = biased_to_float((xr[u1][r] >> sh1) & maskBg, digit_bias);
+                const float b1 = biased_to_float((xr[u1][kR + r] >> sh1) & maskBg, digit_bias);
+                z[r] = {make_float2(a0, b0), make_float2(-a1, -b1)};
+            }
+            F2::forward(z, xp, s_tw2, t, bar_id);
+            // spectrum words in multiply-accumulate order: per register pair m, re(2m), re(2m+1),
+            // im(2m), im(2m+1); digit d0 then digit d0 + 1
+            uint32_t w[32];
+#pragma unroll
+            for (int m = 0; m < kR / 2; m++) {
+                w[4 * m + 0] = __float_as_uint(z[2 * m].re.x);
+                w[4 * m + 1] = __float_as_uint(z[2 * m + 1].re.x);
+                w[4 * m + 2] = __float_as_uint(z[2 * m].im.x);
+                w[4 * m + 3] = __float_as_uint(z[2 * m + 1].im.x);
+                w[16 + 4 * m + 0] = __float_as_uint(z[2 * m].re.y);
+                w[16 + 4 * m + 1] = __float_as_uint(z[2 * m + 1].re.y);
+                w[16 + 4 * m + 2] = __float_as_uint(z[2 * m].im.y);
+                w[16 + 4 * m + 3] = __float_as_uint(z[2 * m + 1].im.y);
+            }
+            tmem_st32(tmem_row + (uint32_t)(d0 * 16), w);
+        }
+        tmem_wait_st();
+
+        // 3. per output polynomial: multiply-accumulate over the digits against the key half rows,
+        //    then both limbs' inverse transforms together, exact rounding, accumulate
+#pragma unroll 1
+        for (int v = 0; v < KP1; v++) {
+            cpair ah[kR / 2], al[kR / 2];
+#pragma unroll
+            for (int m = 0; m < kR / 2; m++) {
+                ah[m] = {{0.f, 0.f}, {0.f, 0.f}};
+                al[m] = {{0.f, 0.f}, {0.f, 0.f}};
+            }
+#pragma unroll 1
+            for (int d = 0; d < KPL; d++) {
+                const int c = (step * KP1 + v) * KPL + d, s = c % D;
+                uint32_t f[16];
+                tmem_ld16(tmem_row + (uint32_t)(d * 16), f);
+                wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns, args.err);
+                // half row: [m][limb][t] x float4 {re(2m), re(2m+1), im(2m), im(2m+1)}
+                const float4 *kp = reinterpret_cast<const float4 *>(smem + Lay::ring + (size_t)s * Lay::half) + t;
+#pragma unroll
+                for (int m = 0; m < kR / 2; m++) {
+                    const cpair zp{make_float2(__uint_as_float(f[4 * m]), __uint_as_float(f[4 * m + 1])),
+                                   make_float2(__uint_as_float(f[4 * m + 2]), __uint_as_float(f[4 * m + 3]))};
+                    const float2 nzi = mul2(zp.im, make_float2(-1.f, -1.f));
+                    cmac_pair(ah[m], zp, nzi, kp[(2 * m) * NT]);
+                    cmac_pair(al[m], zp, nzi, kp[(2 * m + 1) * NT]);
+                }
+                mbar_arrive(empty_bar(s));
+            }
+            // (hi, lo) per slot for the paired inverse
+            cpair x[kR];
+#pragma unroll
+            for (int m = 0; m < kR / 2; m++) {
+                x[2 * m] = {make_float2(ah[m].re.x, al[m].re.x), make_float2(ah[m].im.x, al[m].im.x)};
+                x[2 * m + 1] = {make_float2(ah[m].re.y, al[m].re.y), make_float2(ah[m].im.y, al[m].im.y)};
+            }
+            F2::inverse(x, xp, s_tw2, t, bar_id);
+            uint32_t *poly = s_acc + v * N;
+#pragma unroll
+            for (int r = 0; r < kR; r++) {  // (c_j - i c_{j+M}) of each limb, the high limb weighted 2^S
+                const int j = t + NT * r;
+                poly[j] += (round_f32_mod32(x[r].re.x) << args.split_shift) + (uint32_t)__float2ll_rn(x[r].re.y);
+                poly[j + M] += (round_f32_mod32(-x[r].im.x) << args.split_shift) + (uint32_t)__float2ll_rn(-x[r].im.y);
+            }
+        }
+        team_sync(bar_id, NT);
+    }
+
+    uint32_t *dst = reinterpret_cast<uint32_t *>(args.acc_out) + (size_t)boot * KP1 * N;
+    for (int i = t; i < KP1 * N; i += NT) dst[i] = s_acc[i];
+
+    // every consumer's TMEM accesses are complete (each load waited; stores waited per step)
+    tmem_fence_before_sync();
+    team_sync(kAllBar, active_teams * NT);
+    tmem_fence_after_sync();
+    __syncwarp();
+    if (warp == 0) tmem_free(tmem_base, Lay::tmem_cols);
+}
+
+template <int N, int L, int G, int D, int XB>
+cudaError_t launch_paired(const BrArgs &a, cudaStream_t s) {
+    using Lay = PairLayout<N, L, G, D, XB>;
+    if (!a.tables2) return cudaErrorInvalidValue;
+    auto kern = blind_rotate_paired_kernel<N, L, G, D, XB>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::bytes);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.boots + G - 1) / G;
+    kern<<<grid, Lay::threads, Lay::bytes, s>>>(a);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_paired<1024, 3, 7, 8, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<1024, 3, 7, 4, 2>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<1024, 3, 6, 6, 2>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<2048, 3, 2, 4, 2>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<2048, 3, 2, 6, 2>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<2048, 3, 3, 4, 1>(const BrArgs &, cudaStream_t);
+
+}  // namespace tfheb

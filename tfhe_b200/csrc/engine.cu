@@ -150,9 +150,11 @@ static cudaError_t timed(CloudKey &ck, int which, cudaStream_t s, Fn &&fn) {
     return e;
 }
 
-// Device pipeline for `count` gates described by (bd, gd) already uploaded.
+// Device pipeline for `count` gates described by (bd, gd) already uploaded.  d_terms (optional):
+// per gate, the keyswitch's non-zero digit count.
 static tfheb_status run_pipeline(CloudKey &ck, int precision, int count, int boots, const int32_t *d_a,
-                                 const int32_t *d_b, const int32_t *d_c, int32_t *d_out, cudaStream_t s) {
+                                 const int32_t *d_b, const int32_t *d_c, int32_t *d_out, cudaStream_t s,
+                                 int32_t *d_terms) {
     const tfheb_params &p = ck.p;
     const int bs = bara_stride_of(p);
     const int kN1 = p.k * p.N + 1;
@@ -172,6 +174,10 @@ static tfheb_status run_pipeline(CloudKey &ck, int precision, int count, int boo
     }));
     g_launches += 4;
     ck.launches += 4;
+    if (d_terms) {
+        TFHEB_CUDA(launch_ks_terms(p, count, ck.d_ksin, kN1, d_terms, s));
+        g_launches += 1;
+    }
     return TFHEB_OK;
 }
 
@@ -185,6 +191,16 @@ tfheb_status check_device_error(CloudKey &ck) {
         return TFHEB_ERR_TIMEOUT;
     }
     return TFHEB_OK;
+}
+
+tfheb_status sync_key_stream(tfheb_cloud_key *c) {
+    if (!c) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    if (ck.device < 0) return TFHEB_OK;
+    TFHEB_CUDA(cudaSetDevice(ck.device));
+    TFHEB_CUDA(cudaStreamSynchronize(ck.stream));
+    return check_device_error(ck);
 }
 
 static tfheb_status upload_descs(CloudKey &ck, const std::vector<BootDesc> &bd, const std::vector<GateDesc> &gd,
@@ -247,9 +263,11 @@ static tfheb_status ensure_descs(CloudKey &ck, int gate, int count, cudaStream_t
     return TFHEB_OK;
 }
 
-// `count` gates of one type on device buffers, enqueued on s (the key's lock held).
+// `count` gates of one type on device buffers, enqueued on s (the key's lock held).  d_terms
+// (optional, bootstrapped gates only): per gate, the keyswitch's non-zero digit count.
 static tfheb_status gate_chunk(CloudKey &ck, int gate, int precision, int count, const int32_t *d_a,
-                               const int32_t *d_b, const int32_t *d_c, int32_t *d_out, cudaStream_t s) {
+                               const int32_t *d_b, const int32_t *d_c, int32_t *d_out, cudaStream_t s,
+                               int32_t *d_terms = nullptr) {
     const int n1 = ck.p.n + 1;
     if (gate == TFHEB_COPY || gate == TFHEB_NOT) {
         // bootstrap-free (boot-gates.cpp:164-178)
@@ -261,10 +279,14 @@ static tfheb_status gate_chunk(CloudKey &ck, int gate, int precision, int count,
         g_launches += 1;
         return TFHEB_OK;
     }
+    if (!ck.dksk.rows) {
+        set_error("the cloud key has no keyswitching key");
+        return TFHEB_ERR_INVALID;
+    }
     const tfheb_status st = ensure_descs(ck, gate, count, s);
     if (st != TFHEB_OK) return st;
     const int boots = gate == TFHEB_MUX ? 2 * count : count;
-    return run_pipeline(ck, precision, count, boots, d_a, d_b, d_c, d_out, s);
+    return run_pipeline(ck, precision, count, boots, d_a, d_b, d_c, d_out, s, d_terms);
 }
 
 }  // namespace tfheb
@@ -308,7 +330,7 @@ tfheb_status tfheb_keygen(const tfheb_params *p, uint64_t seed, tfheb_secret_key
 
 tfheb_status tfheb_cloud_key_import(const tfheb_params *p, const int32_t *bsk, const int32_t *ksk,
                                     tfheb_cloud_key **ck) {
-    if (!valid_params(p) || !bsk || !ksk || !ck) {
+    if (!valid_params(p) || !bsk || !ck) {
         set_error("invalid arguments");
         return TFHEB_ERR_INVALID;
     }
@@ -317,7 +339,7 @@ tfheb_status tfheb_cloud_key_import(const tfheb_params *p, const int32_t *bsk, c
     const size_t nb = (size_t)p->n * (p->k + 1) * p->l * (p->k + 1) * p->N;
     const size_t nk = (size_t)p->k * p->N * p->ks_t * (1 << p->ks_basebit) * (p->n + 1);
     c->ck.bsk_coef.assign(bsk, bsk + nb);
-    c->ck.ksk.assign(ksk, ksk + nk);
+    if (ksk) c->ck.ksk.assign(ksk, ksk + nk);  // without one, the key serves blind rotations only
     *ck = c;
     return TFHEB_OK;
 }
@@ -366,12 +388,14 @@ void tfheb_cloud_key_free(tfheb_cloud_key *c) {
         for (auto &d : ck.dbsk) {
             cudaFree(d.bsk);
             cudaFree(d.tables);
+            cudaFree(d.tables2);
         }
         free_keyswitch_key(ck.dksk);
         cudaFree(ck.d_bara);
         cudaFree(ck.d_acc);
         cudaFree(ck.d_ksin);
         cudaFree(ck.d_io);
+        cudaFree(ck.d_terms);
         cudaFree(ck.d_bdesc);
         cudaFree(ck.d_gdesc);
         cudaFree(ck.d_err);
@@ -440,8 +464,9 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32
         TFHEB_CUDA(cudaMemset(ck.d_err, 0, sizeof(int32_t)));
     }
     const tfheb_params &p = ck.p;
-    // keyswitching key in the layouts of both keyswitch kernels
-    TFHEB_CUDA(upload_keyswitch_key(ck));
+    // keyswitching key in the layouts of the keyswitch kernels (absent from keys made for blind
+    // rotations only)
+    if (!ck.ksk.empty()) TFHEB_CUDA(upload_keyswitch_key(ck));
     std::vector<double> tab;
     build_tables_fp64(p.N, tab);
     // the FFT-domain keys are computed on the device (key_transform.cu) from the coefficient key
@@ -460,7 +485,8 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32
         if (d.bsk) {
             cudaFree(d.bsk);
             cudaFree(d.tables);
-            d.bsk = d.tables = nullptr;
+            cudaFree(d.tables2);
+            d.bsk = d.tables = d.tables2 = nullptr;
         }
         if (!d_coef.p) {
             TFHEB_CUDA(cudaMalloc(&d_coef.p, ck.bsk_coef.size() * sizeof(int32_t)));
@@ -482,6 +508,9 @@ tfheb_status tfheb_cloud_key_to_device(tfheb_cloud_key *c, int32_t device, int32
             build_tables_f32(p.N, tf);
             TFHEB_CUDA(cudaMalloc(&d.tables, tf.size() * sizeof(float)));
             TFHEB_CUDA(cudaMemcpy(d.tables, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice));
+            build_tables_f32_paired(p.N, tf);
+            TFHEB_CUDA(cudaMalloc(&d.tables2, tf.size() * sizeof(float)));
+            TFHEB_CUDA(cudaMemcpy(d.tables2, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice));
         }
     }
     TFHEB_CUDA(cudaStreamSynchronize(ck.stream));
@@ -531,8 +560,9 @@ tfheb_status tfheb_gate_batch_device(tfheb_cloud_key *c, int32_t gate, int32_t p
 // unsplit across boxes): the copies it hides (about 0.6 ms per 4096 gates) are offset by what the
 // chunks add, a keyswitch per chunk that streams the keyswitching key through L2 again and evicts
 // part of the bootstrapping key, and a ramp and tail per blind-rotation launch.
-tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precision, int32_t count,
-                              const int32_t *a, const int32_t *b, const int32_t *cc, int32_t *out) {
+static tfheb_status gate_batch_host(tfheb_cloud_key *c, int32_t gate, int32_t precision, int32_t count,
+                                    const int32_t *a, const int32_t *b, const int32_t *cc, int32_t *out,
+                                    int32_t *terms) {
     if (!c || count < 0 || gate < 0 || gate > TFHEB_COPY) return TFHEB_ERR_INVALID;
     if (count == 0) return TFHEB_OK;
     if (!a || !out || (gate == TFHEB_MUX && (!b || !cc)) || (gate < TFHEB_MUX && !b)) return TFHEB_ERR_INVALID;
@@ -542,6 +572,10 @@ tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precisio
     if (st != TFHEB_OK) return st;
     const size_t sz = (size_t)count * (ck.p.n + 1);
     if ((st = grow(ck.d_io, ck.io_cap, 4 * sz)) != TFHEB_OK) return st;
+    const bool with_terms = terms && gate != TFHEB_NOT && gate != TFHEB_COPY;
+    if (terms && !with_terms)
+        for (int32_t g = 0; g < count; g++) terms[g] = -1;  // no keyswitch: the input's variance carries over
+    if (with_terms && (st = grow(ck.d_terms, ck.terms_cap, (size_t)count)) != TFHEB_OK) return st;
     int32_t *dio = ck.d_io;
     cudaStream_t s = ck.stream;
     if ((st = scratch_begin(ck, s)) != TFHEB_OK) return st;
@@ -549,13 +583,27 @@ tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precisio
     if (b) TFHEB_CUDA(cudaMemcpyAsync(dio + sz, b, sz * 4, cudaMemcpyHostToDevice, s));
     if (cc) TFHEB_CUDA(cudaMemcpyAsync(dio + 2 * sz, cc, sz * 4, cudaMemcpyHostToDevice, s));
     st = gate_chunk(ck, gate, precision, count, dio, b ? dio + sz : nullptr, cc ? dio + 2 * sz : nullptr,
-                    dio + 3 * sz, s);
+                    dio + 3 * sz, s, with_terms ? ck.d_terms : nullptr);
     if (st == TFHEB_OK) TFHEB_CUDA(cudaMemcpyAsync(out, dio + 3 * sz, sz * 4, cudaMemcpyDeviceToHost, s));
+    if (st == TFHEB_OK && with_terms)
+        TFHEB_CUDA(cudaMemcpyAsync(terms, ck.d_terms, (size_t)count * 4, cudaMemcpyDeviceToHost, s));
     if (st == TFHEB_OK) st = scratch_end(ck, s);
     const cudaError_t e = cudaStreamSynchronize(s);  // drain, also after an error
     if (st != TFHEB_OK) return st;
     TFHEB_CUDA(e);
     return check_device_error(ck);
+}
+
+tfheb_status tfheb_gate_batch(tfheb_cloud_key *c, int32_t gate, int32_t precision, int32_t count,
+                              const int32_t *a, const int32_t *b, const int32_t *cc, int32_t *out) {
+    return gate_batch_host(c, gate, precision, count, a, b, cc, out, nullptr);
+}
+
+tfheb_status tfheb_gate_batch_terms(tfheb_cloud_key *c, int32_t gate, int32_t precision, int32_t count,
+                                    const int32_t *a, const int32_t *b, const int32_t *cc, int32_t *out,
+                                    int32_t *terms) {
+    if (!terms) return TFHEB_ERR_INVALID;
+    return gate_batch_host(c, gate, precision, count, a, b, cc, out, terms);
 }
 
 // Bootstraps without keyswitch of `count` samples (the key's lock held).
@@ -610,7 +658,10 @@ tfheb_status tfheb_bootstrap_device(tfheb_cloud_key *c, int32_t precision, int32
     CloudKey &ck = c->ck;
     tfheb_status st = ensure_device(ck, precision);
     if (st != TFHEB_OK) return st;
-    if (!ck.dksk.rows) return TFHEB_ERR_INVALID;
+    if (!ck.dksk.rows) {
+        set_error("the cloud key has no keyswitching key");
+        return TFHEB_ERR_INVALID;
+    }
     if (count == 0) return TFHEB_OK;
     if ((st = check_device_ptr(ck, d_in, "d_in")) != TFHEB_OK || (st = check_device_ptr(ck, d_out, "d_out")) != TFHEB_OK)
         return st;
@@ -627,22 +678,121 @@ tfheb_status tfheb_bootstrap_device(tfheb_cloud_key *c, int32_t precision, int32
     return st != TFHEB_OK ? st : se;
 }
 
-tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *c, int32_t precision, int32_t count, int32_t nsteps,
-                                       const int32_t *d_bara, int32_t *d_acc, void *stream) {
-    if (!c || count < 0 || !d_bara || !d_acc || nsteps < 0) return TFHEB_ERR_INVALID;
+// The device key from TGSW step `first` on: every step's rows are contiguous in both layouts.
+static DeviceBsk key_from_step(const CloudKey &ck, int precision, int first) {
+    DeviceBsk d = ck.dbsk[precision];
+    const tfheb_params &p = ck.p;
+    const size_t step_bytes = (size_t)(p.k + 1) * p.l * (p.k + 1) * (p.N / 2) * 16;
+    d.bsk = static_cast<unsigned char *>(d.bsk) + step_bytes * (size_t)first;
+    return d;
+}
+
+tfheb_status tfheb_blind_rotate_steps_device(tfheb_cloud_key *c, int32_t precision, int32_t count, int32_t first_step,
+                                             int32_t nsteps, const int32_t *d_bara, int32_t *d_acc, void *stream) {
+    if (!c || count < 0 || !d_bara || !d_acc || nsteps < 0 || first_step < 0) return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
     CloudKey &ck = c->ck;
-    if (nsteps > ck.p.n) return TFHEB_ERR_INVALID;
+    if ((int64_t)first_step + nsteps > ck.p.n) {
+        set_error("blind rotation: steps beyond the key's " + std::to_string(ck.p.n) + " TGSW samples");
+        return TFHEB_ERR_INVALID;
+    }
     tfheb_status st = ensure_device(ck, precision);
     if (st != TFHEB_OK) return st;
-    if (count == 0) return TFHEB_OK;
+    if (count == 0 || nsteps == 0) return TFHEB_OK;
     if ((st = check_device_ptr(ck, d_bara, "d_bara")) != TFHEB_OK || (st = check_device_ptr(ck, d_acc, "d_acc")) != TFHEB_OK)
         return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
     // in place: acc_in == acc_out is safe (each team reads its row fully before writing it back)
-    TFHEB_CUDA(launch_blind_rotate(ck.p, precision, ck.dbsk[precision], d_bara, nsteps, count, nsteps, 0, d_acc,
-                                   d_acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns,
+    TFHEB_CUDA(launch_blind_rotate(ck.p, precision, key_from_step(ck, precision, first_step), d_bara, nsteps, count,
+                                   nsteps, 0, d_acc, d_acc, s, ck.d_err, ck.stall_producer, ck.wait_timeout_ns,
                                    ck.br[precision]));
+    g_launches += 1;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_blind_rotate_device(tfheb_cloud_key *c, int32_t precision, int32_t count, int32_t nsteps,
+                                       const int32_t *d_bara, int32_t *d_acc, void *stream) {
+    return tfheb_blind_rotate_steps_device(c, precision, count, 0, nsteps, d_bara, d_acc, stream);
+}
+
+tfheb_status tfheb_blind_rotate_extract_device(tfheb_cloud_key *c, int32_t precision, int32_t count,
+                                               int32_t first_step, int32_t nsteps, const int32_t *d_v,
+                                               const int32_t *d_barb, const int32_t *d_bara, int32_t *d_out,
+                                               void *stream) {
+    if (!c || count < 0 || nsteps < 0 || first_step < 0) return TFHEB_ERR_INVALID;
+    if (count > 0 && (!d_v || !d_barb || !d_out || (nsteps > 0 && !d_bara))) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    const tfheb_params &p = ck.p;
+    if ((int64_t)first_step + nsteps > p.n) {
+        set_error("blind rotation: steps beyond the key's " + std::to_string(p.n) + " TGSW samples");
+        return TFHEB_ERR_INVALID;
+    }
+    tfheb_status st = ensure_device(ck, precision);
+    if (st != TFHEB_OK) return st;
+    if (count == 0) return TFHEB_OK;
+    for (auto [ptr, what] : {std::pair<const void *, const char *>{d_v, "d_v"}, {d_barb, "d_barb"}, {d_bara, "d_bara"},
+                             {d_out, "d_out"}})
+        if ((st = check_device_ptr(ck, ptr, what)) != TFHEB_OK) return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+    if ((st = scratch_begin(ck, s)) != TFHEB_OK) return st;
+    if ((st = grow(ck.d_acc, ck.acc_cap, (size_t)count * (p.k + 1) * p.N)) == TFHEB_OK) {
+        cudaError_t e = launch_testvec(p, count, d_v, d_barb, ck.d_acc, s);
+        if (e == cudaSuccess && nsteps > 0)
+            e = launch_blind_rotate(p, precision, key_from_step(ck, precision, first_step), d_bara, nsteps, count,
+                                    nsteps, 0, ck.d_acc, ck.d_acc, s, ck.d_err, ck.stall_producer,
+                                    ck.wait_timeout_ns, ck.br[precision]);
+        if (e == cudaSuccess) e = launch_extract(p, nullptr, count, ck.d_acc, d_out, p.k * p.N + 1, s);
+        if (e != cudaSuccess) st = cuda_fail(e, "tfheb_blind_rotate_extract_device");
+        g_launches += nsteps > 0 ? 3 : 2;
+    }
+    const tfheb_status se = scratch_end(ck, s);
+    return st != TFHEB_OK ? st : se;
+}
+
+tfheb_status tfheb_extern_product_device(tfheb_cloud_key *c, int32_t precision, int32_t count, int32_t step,
+                                         const int32_t *d_in, int32_t *d_out, void *stream) {
+    if (!c || count < 0 || step < 0) return TFHEB_ERR_INVALID;
+    if (count > 0 && (!d_in || !d_out)) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    if (step >= ck.p.n) {
+        set_error("external product: the key has " + std::to_string(ck.p.n) + " TGSW samples");
+        return TFHEB_ERR_INVALID;
+    }
+    tfheb_status st = ensure_device(ck, precision);
+    if (st != TFHEB_OK) return st;
+    if (count == 0) return TFHEB_OK;
+    if ((st = check_device_ptr(ck, d_in, "d_in")) != TFHEB_OK || (st = check_device_ptr(ck, d_out, "d_out")) != TFHEB_OK)
+        return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+    const cudaError_t e = launch_extern_product(ck.p, precision, key_from_step(ck, precision, step), count, d_in, d_out,
+                                                s, ck.d_err, ck.wait_timeout_ns);
+    if (e == cudaErrorInvalidValue) {
+        set_error("external product: no compiled kernel for this ring degree and gadget length");
+        return TFHEB_ERR_UNSUPPORTED;
+    }
+    TFHEB_CUDA(e);
+    g_launches += 1;
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_ks_terms_device(tfheb_cloud_key *c, int32_t count, const int32_t *d_in, int32_t *d_terms,
+                                   void *stream) {
+    if (!c || count < 0 || (count > 0 && (!d_in || !d_terms))) return TFHEB_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(c->mu);
+    CloudKey &ck = c->ck;
+    if (ck.device < 0) {
+        set_error("cloud key is not on a device (call tfheb_cloud_key_to_device)");
+        return TFHEB_ERR_INVALID;
+    }
+    TFHEB_CUDA(cudaSetDevice(ck.device));
+    if (count == 0) return TFHEB_OK;
+    tfheb_status st;
+    if ((st = check_device_ptr(ck, d_in, "d_in")) != TFHEB_OK || (st = check_device_ptr(ck, d_terms, "d_terms")) != TFHEB_OK)
+        return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ck.stream;
+    TFHEB_CUDA(launch_ks_terms(ck.p, count, d_in, ck.p.k * ck.p.N + 1, d_terms, s));
     g_launches += 1;
     return TFHEB_OK;
 }
@@ -652,7 +802,10 @@ tfheb_status tfheb_keyswitch_device(tfheb_cloud_key *c, int32_t count, const int
     if (!c || count < 0 || !d_in || !d_out) return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
     CloudKey &ck = c->ck;
-    if (ck.device < 0 || !ck.dksk.rows) return TFHEB_ERR_INVALID;
+    if (ck.device < 0 || !ck.dksk.rows) {
+        set_error("the cloud key has no keyswitching key on a device");
+        return TFHEB_ERR_INVALID;
+    }
     TFHEB_CUDA(cudaSetDevice(ck.device));
     if (count == 0) return TFHEB_OK;
     tfheb_status st;
@@ -693,6 +846,13 @@ tfheb_status tfheb_cloud_key_br_variants(const tfheb_cloud_key *c, int32_t preci
                                          int32_t *ring_depth, int32_t cap, int32_t *count) {
     if (!c || !count || cap < 0) return TFHEB_ERR_INVALID;
     *count = br_variants(c->ck.p.N, c->ck.p.l, precision, teams_per_cta, ring_depth, cap);
+    return TFHEB_OK;
+}
+
+tfheb_status tfheb_cloud_key_br_plans(const tfheb_cloud_key *c, int32_t precision, int32_t *plan, int32_t cap,
+                                      int32_t *count) {
+    if (!c || !count || cap < 0) return TFHEB_ERR_INVALID;
+    *count = br_variant_plans(c->ck.p.N, c->ck.p.l, precision, plan, cap);
     return TFHEB_OK;
 }
 

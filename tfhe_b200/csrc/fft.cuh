@@ -571,4 +571,208 @@ struct TeamFft {
     }
 };
 
+// ---- two transforms per thread on packed f32x2 --------------------------------------------------
+// TeamFft2 runs two independent FP32 transforms of the same size in lockstep: register r of a thread
+// holds point r of transform A in the .x halves and of transform B in the .y halves of a cpair.
+// Every packed instruction performs, on each half, the scalar operation that TeamFft<float> performs
+// at the same place (same operands, same rounding, same order; negations are exact), so each
+// transform's result is TeamFft<float>'s bit for bit, with half the FP32 instructions issued.
+// Twiddles come from a table of broadcast pairs {w.re, w.re, w.im, w.im} holding the scalar FP32
+// table's factors (tw2_entries: the FP64 table's layout, tw_offset); the exchange moves one 16-byte
+// {A.re, B.re, A.im, B.im} per point under the 16-byte layout of Exch<double, M>.
+
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    float2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;"
+        : "=l"(*reinterpret_cast<unsigned long long *>(&d))
+        : "l"(*reinterpret_cast<const unsigned long long *>(&a)), "l"(*reinterpret_cast<const unsigned long long *>(&b)));
+    return d;
+}
+__device__ __forceinline__ float2 neg2(float2 a) { return mul2(a, make_float2(-1.f, -1.f)); }  // exact
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ cpair padd(const cpair &a, const cpair &b) { return {add2(a.re, b.re), add2(a.im, b.im)}; }
+__device__ __forceinline__ cpair psub(const cpair &a, const cpair &b) { return {sub2(a.re, b.re), sub2(a.im, b.im)}; }
+
+// cmul / cmulconj of both halves by one factor w = (wr, wi) given as broadcast pairs, with nwi = -wi
+// (x * (-y) = -(x * y) exactly, so the negated product costs no instruction)
+__device__ __forceinline__ cpair pmul(const cpair &a, float2 wr, float2 wi, float2 nwi) {
+    // {fma(a.re, w.re, -(a.im * w.im)), fma(a.re, w.im, a.im * w.re)}
+    return {fma2(a.re, wr, mul2(a.im, nwi)), fma2(a.re, wi, mul2(a.im, wr))};
+}
+__device__ __forceinline__ cpair pmulconj(const cpair &a, float2 wr, float2 wi, float2 nwi) {
+    // {fma(a.re, w.re, a.im * w.im), fma(a.im, w.re, -(a.re * w.im))}
+    return {fma2(a.re, wr, mul2(a.im, wi)), fma2(a.im, wr, mul2(a.re, nwi))};
+}
+
+// dft4 of TeamFft on both halves; the quarter rotation is folded into which pair is added or
+// subtracted (x + (-y) and x - y are the same IEEE operation)
+template <bool INV>
+__device__ __forceinline__ void pdft4(cpair &x0, cpair &x1, cpair &x2, cpair &x3) {
+    const cpair s02 = padd(x0, x2), d02 = psub(x0, x2);
+    const cpair s13 = padd(x1, x3), s = psub(x1, x3);
+    x0 = padd(s02, s13);
+    x2 = psub(s02, s13);
+    if (!INV) {  // d13 = (s.im, -s.re)
+        x1 = {add2(d02.re, s.im), sub2(d02.im, s.re)};
+        x3 = {sub2(d02.re, s.im), add2(d02.im, s.re)};
+    } else {     // d13 = (-s.im, s.re)
+        x1 = {sub2(d02.re, s.im), add2(d02.im, s.re)};
+        x3 = {add2(d02.re, s.im), sub2(d02.im, s.re)};
+    }
+}
+
+template <bool INV>
+__device__ __forceinline__ void pdft8(cpair *x) {
+    cpair e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6];
+    cpair o0 = x[1], o1 = x[3], o2 = x[5], o3 = x[7];
+    pdft4<INV>(e0, e1, e2, e3);
+    pdft4<INV>(o0, o1, o2, o3);
+    const float2 h = bc2(rsqrt2<float>()), nh = bc2(-rsqrt2<float>());
+    x[0] = padd(e0, o0);
+    x[4] = psub(e0, o0);
+    if (!INV) {
+        // u1 = o1.re + o1.im, v1 = o1.im - o1.re, u3 = o3.im - o3.re, v3 = -(o3.re + o3.im)
+        const float2 u1 = add2(o1.re, o1.im), v1 = sub2(o1.im, o1.re);
+        const float2 u3 = sub2(o3.im, o3.re), p3 = add2(o3.re, o3.im);
+        x[1] = {fma2(u1, h, e1.re), fma2(v1, h, e1.im)};
+        x[5] = {fma2(u1, nh, e1.re), fma2(v1, nh, e1.im)};
+        x[3] = {fma2(u3, h, e3.re), fma2(p3, nh, e3.im)};
+        x[7] = {fma2(u3, nh, e3.re), fma2(p3, h, e3.im)};
+        // w2 = (o2.im, -o2.re)
+        x[2] = {add2(e2.re, o2.im), sub2(e2.im, o2.re)};
+        x[6] = {sub2(e2.re, o2.im), add2(e2.im, o2.re)};
+    } else {
+        // u1 = o1.re - o1.im, v1 = o1.re + o1.im, u3 = -(o3.re + o3.im), v3 = o3.re - o3.im
+        const float2 u1 = sub2(o1.re, o1.im), v1 = add2(o1.re, o1.im);
+        const float2 p3 = add2(o3.re, o3.im), v3 = sub2(o3.re, o3.im);
+        x[1] = {fma2(u1, h, e1.re), fma2(v1, h, e1.im)};
+        x[5] = {fma2(u1, nh, e1.re), fma2(v1, nh, e1.im)};
+        x[3] = {fma2(p3, nh, e3.re), fma2(v3, h, e3.im)};
+        x[7] = {fma2(p3, h, e3.re), fma2(v3, nh, e3.im)};
+        // w2 = (-o2.im, o2.re)
+        x[2] = {sub2(e2.re, o2.im), add2(e2.im, o2.re)};
+        x[6] = {add2(e2.re, o2.im), sub2(e2.im, o2.re)};
+    }
+}
+
+template <int M>
+struct TeamFft2 {
+    static constexpr int R = 8, NT = M / R, NS = FftPlan<M>::NS;
+    using Scalar = TeamFft<double, M, 8>;  // positions and the 16-byte exchange layout
+    static_assert(FftPlan<M>::radix(0) == 8, "stage 0 is the thread's own radix-8 DFT");
+
+    template <bool INV, int RADIX>
+    __device__ static __forceinline__ void pdft(cpair *x) {
+        if constexpr (RADIX == 8) pdft8<INV>(x);
+        else if constexpr (RADIX == 4) pdft4<INV>(x[0], x[1], x[2], x[3]);
+        else {
+            const cpair a = x[0], b = x[1];
+            x[0] = padd(a, b);
+            x[1] = psub(a, b);
+        }
+    }
+
+    template <int S, int E>
+    __device__ static __forceinline__ void store(const cpair *x, void *buf, int t) {
+        constexpr int r = Stage<M, S>::r;
+        const int base = Scalar::xindex(E, Scalar::template pos<S>(t, 0, 0));
+        float4 *b = reinterpret_cast<float4 *>(buf);
+#pragma unroll
+        for (int c = 0; c < R / r; c++)
+#pragma unroll
+            for (int n2 = 0; n2 < r; n2++) {
+                const cpair &v = x[c * r + n2];
+                b[base + Scalar::template delta<S, E>(c, n2)] = make_float4(v.re.x, v.re.y, v.im.x, v.im.y);
+            }
+    }
+    template <int S, int E>
+    __device__ static __forceinline__ void load(cpair *x, const void *buf, int t) {
+        constexpr int r = Stage<M, S>::r;
+        const int base = Scalar::xindex(E, Scalar::template pos<S>(t, 0, 0));
+        const float4 *b = reinterpret_cast<const float4 *>(buf);
+#pragma unroll
+        for (int c = 0; c < R / r; c++)
+#pragma unroll
+            for (int n2 = 0; n2 < r; n2++) {
+                const float4 v = b[base + Scalar::template delta<S, E>(c, n2)];
+                x[c * r + n2] = {make_float2(v.x, v.y), make_float2(v.z, v.w)};
+            }
+    }
+
+    // stage S's twiddles from the broadcast table (layout of tw_offset, one float4 per factor)
+    template <int S, bool INV>
+    __device__ static __forceinline__ void twiddle(cpair *x, const float4 *tw2, int t) {
+        constexpr int r = Stage<M, S>::r, st = Stage<M, S>::stride;
+        auto apply = [&](cpair &v, float4 w) {
+            const float2 wr = make_float2(w.x, w.y), wi = make_float2(w.z, w.w);
+            v = INV ? pmulconj(v, wr, wi, neg2(wi)) : pmul(v, wr, wi, neg2(wi));
+        };
+        if constexpr (S == 0) {
+#pragma unroll
+            for (int k2 = 0; k2 < r; k2++) apply(x[k2], tw2[k2 * NT + t]);
+        } else if constexpr (st > 1) {
+            const float4 *tws = tw2 + tw_offset<M>(S);
+#pragma unroll
+            for (int c = 0; c < R / r; c++) {
+                const int n1 = (t + NT * c) % st;
+#pragma unroll
+                for (int k2 = 1; k2 < r; k2++) apply(x[c * r + k2], tws[(k2 - 1) * st + n1]);
+            }
+        }
+    }
+
+    // x[n] *= exp(-+ i pi n / 16): TeamFft::fold_consts with w = (cos, -sin) as float constants
+    template <bool INV>
+    __device__ static __forceinline__ void fold_consts(cpair *x) {
+#pragma unroll
+        for (int n = 1; n < R; n++) {
+            const float wr = float(fold_cos(n)), wi = float(-fold_sin(n));
+            x[n] = INV ? pmulconj(x[n], bc2(wr), bc2(wi), bc2(-wi)) : pmul(x[n], bc2(wr), bc2(wi), bc2(-wi));
+        }
+    }
+
+    template <int S>
+    __device__ static __forceinline__ void forward_from(cpair *x, ExchPair &xp, const float4 *tw2, int t, int bar_id) {
+        constexpr int r = Stage<M, S>::r;
+#pragma unroll
+        for (int c = 0; c < R / r; c++) pdft<false, r>(x + c * r);
+        twiddle<S, false>(x, tw2, t);
+        if constexpr (S + 1 < NS) {
+            void *buf = xp.next();
+            store<S, S>(x, buf, t);
+            team_sync(bar_id, NT);
+            load<S + 1, S>(x, buf, t);
+            if (xp.stride == 0) team_sync(bar_id, NT);
+            forward_from<S + 1>(x, xp, tw2, t, bar_id);
+        }
+    }
+    template <int S>
+    __device__ static __forceinline__ void inverse_from(cpair *x, ExchPair &xp, const float4 *tw2, int t, int bar_id) {
+        constexpr int r = Stage<M, S>::r;
+        twiddle<S, true>(x, tw2, t);
+#pragma unroll
+        for (int c = 0; c < R / r; c++) pdft<true, r>(x + c * r);
+        if constexpr (S > 0) {
+            void *buf = xp.next();
+            store<S, S - 1>(x, buf, t);
+            team_sync(bar_id, NT);
+            load<S - 1, S - 1>(x, buf, t);
+            if (xp.stride == 0) team_sync(bar_id, NT);
+            inverse_from<S - 1>(x, xp, tw2, t, bar_id);
+        }
+    }
+    // TeamFft::forward on both halves.  In: x[n2] = a_j - i a_{j+M} of each transform.
+    __device__ static __forceinline__ void forward(cpair *x, ExchPair &xp, const float4 *tw2, int t, int bar_id) {
+        fold_consts<false>(x);
+        forward_from<0>(x, xp, tw2, t, bar_id);
+    }
+    // TeamFft::inverse on both halves.
+    __device__ static __forceinline__ void inverse(cpair *x, ExchPair &xp, const float4 *tw2, int t, int bar_id) {
+        inverse_from<NS - 1>(x, xp, tw2, t, bar_id);
+        fold_consts<true>(x);
+    }
+};
+
 }  // namespace tfheb

@@ -285,7 +285,32 @@ void tables_f32_m(std::vector<float> &tf) {
     }
 }
 
+template <int M>
+void tables_f32_paired_m(std::vector<float> &tf) {
+    std::vector<double> tab;
+    tables_m<M>(tab);
+    const size_t n = tab.size() / 2;
+    tf.assign(4 * n, 0.f);
+    for (size_t i = 0; i < n; i++) {
+        const float re = (float)tab[2 * i], im = (float)tab[2 * i + 1];  // the values of tables_f32_m
+        tf[4 * i] = re;
+        tf[4 * i + 1] = re;
+        tf[4 * i + 2] = im;
+        tf[4 * i + 3] = im;
+    }
+}
+
 }  // namespace
+
+void build_tables_f32_paired(int N, std::vector<float> &tab) {
+    switch (N / 2) {
+        case 64: tables_f32_paired_m<64>(tab); break;
+        case 256: tables_f32_paired_m<256>(tab); break;
+        case 512: tables_f32_paired_m<512>(tab); break;
+        case 1024: tables_f32_paired_m<1024>(tab); break;
+        default: tab.clear();
+    }
+}
 
 void fill_slot_freq(int N, std::vector<int32_t> &sf) {
     switch (N / 2) {

@@ -36,6 +36,7 @@ struct GateDesc {
 struct DeviceBsk {
     void *bsk = nullptr;      // [n][kpl][k+1][R][NT] x 16 bytes (double2, or float4 = hi.re,hi.im,lo.re,lo.im)
     void *tables = nullptr;   // stage twiddles (stage 0 carries the twist), layout of the precision
+    void *tables2 = nullptr;  // split only: the FP32 factors as broadcast pairs (build_tables_f32_paired)
     size_t bsk_bytes = 0;
     int split_shift = 0;      // split mode: weight of the high limb is 2^split_shift
 };
@@ -94,6 +95,8 @@ struct CloudKey {
     size_t ksin_cap = 0;
     int32_t *d_io = nullptr;        // device copies of host batches: a,b,c,out
     size_t io_cap = 0;
+    int32_t *d_terms = nullptr;     // keyswitch term counts of a host batch (tfheb_gate_batch_terms)
+    size_t terms_cap = 0;
     cudaEvent_t scratch_done = nullptr;  // the last call using the scratch above finished with it
     BootDesc *d_bdesc = nullptr;
     size_t bdesc_cap = 0;
@@ -136,6 +139,8 @@ int32_t modswitch_from_torus32(int32_t phase, int32_t msize);
 // FFT-domain key preparation (host FP64), layout-compatible with the kernels.
 void build_tables_fp64(int N, std::vector<double> &tables);  // complex pairs (re,im)
 void build_tables_f32(int N, std::vector<float> &tables);    // float4 pairs of factors (tw4_offset)
+// the same FP32 factors as {re, re, im, im} per factor, in the FP64 table's order (tw_offset)
+void build_tables_f32_paired(int N, std::vector<float> &tables);
 void fill_slot_freq(int N, std::vector<int32_t> &slot_freq); // [R][NT] -> frequency index
 // key_transform.cu: coefficient-domain bootstrapping key [n][kpl][k+1][N] on the device -> the
 // FFT-domain layout of `precision` (d_out: n*kpl*(k+1)*N/2*16 bytes), on stream s.
@@ -157,12 +162,33 @@ cudaError_t launch_blind_rotate_exact(const tfheb_params &p, int precision, cons
 // Size of the whole compiled table and one entry's shape; tuned = an autotuner candidate.
 int br_variant_count();
 void br_variant_info(int global_index, int *N, int *l, int *precision, int *G, int *D, int *tuned);
+// FFT plan of a compiled variant: 0 = one transform per thread (radix-8 team FFT), 1 = two transforms
+// per thread on packed f32x2 with the digit spectra in tensor memory (split-FP32 only)
+int br_variant_plan(int global_index);
+// Plans of the launch variants of (N, l, precision), in the order of br_variants.
+int br_variant_plans(int N, int l, int precision, int *plan, int cap);
 // Index into the whole table of the `tuned`-th autotuner candidate of (N, l, precision), or -1.
 int br_tuned_global(int N, int l, int precision, int tuned);
 // Launch variants compiled for (N, l, precision): count, and their (G, D) into the arrays (up to cap).
 int br_variants(int N, int l, int precision, int *G, int *D, int cap);
+// d_desc == nullptr: row g is the plain extraction of accumulator g (no MUX term, no constant)
 cudaError_t launch_extract(const tfheb_params &p, const GateDesc *d_desc, int count, const int32_t *acc,
                            int32_t *out, int out_stride, cudaStream_t s);
+// acc[g] = (0, X^{2N - barb[g]} * v[g]): v [count][N], acc [count][k+1][N]
+cudaError_t launch_testvec(const tfheb_params &p, int count, const int32_t *v, const int32_t *barb, int32_t *acc,
+                           cudaStream_t s);
+// terms[g] = number of non-zero keyswitch digits of extracted sample g (rows of in_stride int32)
+cudaError_t launch_ks_terms(const tfheb_params &p, int count, const int32_t *in, int in_stride, int32_t *terms,
+                            cudaStream_t s);
+// out[g] = bsk_0 (x) in[g] (the first TGSW sample of `bsk`, which the caller may offset to any step):
+// in/out [count][k+1][N]
+cudaError_t launch_extern_product(const tfheb_params &p, int precision, const DeviceBsk &bsk, int count,
+                                  const int32_t *in, int32_t *out, cudaStream_t s, int32_t *d_err,
+                                  uint64_t timeout_ns);
+// blind_rotate_paired.cu: the split-FP32 variants with two transforms per thread (plan 1)
+struct BrArgs;
+template <int N, int L, int G, int D, int XB>
+cudaError_t launch_paired(const BrArgs &a, cudaStream_t s);
 // keyswitch.cu: device key upload (both layouts) and the keyswitch of `count` extracted samples
 // (rows of in_stride int32) into rows of n+1 int32.
 cudaError_t upload_keyswitch_key(CloudKey &ck);
@@ -189,6 +215,8 @@ tfheb_status check_device_error(CloudKey &ck);
 // key's GPU.
 tfheb_status check_device_ptr(const CloudKey &ck, const void *ptr, const char *what);
 extern std::atomic<int64_t> g_kernel_launches;
+// Waits for the key's own stream (not the whole device) and reports a device-side wait that ran out.
+tfheb_status sync_key_stream(tfheb_cloud_key *c);
 
 // ---- reference file format (io.cu) ----------------------------------------------------------
 namespace io {

@@ -176,6 +176,7 @@ bool read_params(FILE *f, tfheb_params &p, ParamMeta &m) {
 
 bool write_cloud_content(FILE *f, const CloudKey &ck) {
     const tfheb_params &p = ck.p;
+    if (ck.ksk.empty()) return fail("the cloud key has no keyswitching key to save");
     Section s{"LWEKSPARAMS",
               {{"n", fmt_int((int64_t)p.k * p.N)}, {"t", fmt_int(p.ks_t)}, {"basebit", fmt_int(p.ks_basebit)}}};
     const double ks_var = ck.ks_var >= 0 ? ck.ks_var : p.ks_stdev * p.ks_stdev;

@@ -54,10 +54,11 @@ cudaError_t launch_prologue(const tfheb_params &p, const BootDesc *d_desc, int b
 // sample extraction (+ MUX recombination)
 // ============================================================================================
 
-// one CTA per gate; out row = extract(acc[boot0]) (+ extract(acc[boot1])) + (0, cst)
+// one CTA per gate; out row = extract(acc[boot0]) (+ extract(acc[boot1])) + (0, cst); without
+// descriptors, row g is the plain extraction of accumulator g
 __global__ void extract_kernel(const GateDesc *__restrict__ desc, const uint32_t *__restrict__ acc, int N, int k,
                                uint32_t *__restrict__ out, int out_stride) {
-    const GateDesc d = desc[blockIdx.x];
+    const GateDesc d = desc ? desc[blockIdx.x] : GateDesc{(int32_t)blockIdx.x, -1, 0};
     const int kN = k * N;
     const size_t tl = (size_t)(k + 1) * N;
     const uint32_t *a0 = acc + (size_t)d.boot0 * tl;
@@ -86,6 +87,70 @@ cudaError_t launch_extract(const tfheb_params &p, const GateDesc *d_desc, int co
     if (count <= 0) return cudaSuccess;
     extract_kernel<<<count, 256, 0, s>>>(d_desc, reinterpret_cast<const uint32_t *>(acc), p.N, p.k,
                                          reinterpret_cast<uint32_t *>(out), out_stride);
+    return cudaGetLastError();
+}
+
+// ============================================================================================
+// test vector of tfhe_blindRotateAndExtract_FFT (lwe-bootstrapping-functions-fft.cpp:142-145):
+// acc = (0, X^{2N - barb} * v) for each sample's own polynomial v and barb
+// ============================================================================================
+
+__global__ void testvec_kernel(const uint32_t *__restrict__ v, const int32_t *__restrict__ barb, int N, int k,
+                               uint32_t *__restrict__ acc) {
+    const int g = blockIdx.x;
+    const uint32_t *vg = v + (size_t)g * N;
+    uint32_t *a = acc + (size_t)g * (k + 1) * N;
+    const int e = (2 * N - (barb[g] & (2 * N - 1))) & (2 * N - 1);  // rotation exponent in [0, 2N)
+    for (int i = threadIdx.x; i < k * N; i += blockDim.x) a[i] = 0u;
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        // (X^e v)_j = +-v_{(j - e) mod N}, negated once per wrap past X^N = -1
+        int src = j - e;
+        uint32_t neg = 0;
+        while (src < 0) {
+            src += N;
+            neg ^= 1u;
+        }
+        a[k * N + j] = neg ? 0u - vg[src] : vg[src];
+    }
+}
+
+cudaError_t launch_testvec(const tfheb_params &p, int count, const int32_t *v, const int32_t *barb, int32_t *acc,
+                           cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    testvec_kernel<<<count, 256, 0, s>>>(reinterpret_cast<const uint32_t *>(v), barb, p.N, p.k,
+                                         reinterpret_cast<uint32_t *>(acc));
+    return cudaGetLastError();
+}
+
+// ============================================================================================
+// keyswitch terms: per extracted sample, how many keyswitching-key rows lweKeySwitch subtracts (the
+// non-zero digits, lwe-keyswitch-functions.cpp:114-129).  The reference's result variance is the
+// sum of those rows' variances; the drop-in reproduces it from this count.
+// ============================================================================================
+
+__global__ void ks_terms_kernel(const uint32_t *__restrict__ in, int in_stride, int kN, int t, int basebit,
+                                int32_t *__restrict__ terms) {
+    __shared__ int total;
+    if (threadIdx.x == 0) total = 0;
+    __syncthreads();
+    const uint32_t *x = in + (size_t)blockIdx.x * in_stride;
+    const uint32_t prec_offset = 1u << (32 - (1 + basebit * t));
+    const uint32_t mask = (1u << basebit) - 1u;
+    int cnt = 0;
+    for (int i = threadIdx.x; i < kN; i += blockDim.x) {
+        const uint32_t aibar = x[i] + prec_offset;
+        for (int j = 0; j < t; j++) cnt += ((aibar >> (32 - (j + 1) * basebit)) & mask) != 0u;
+    }
+    atomicAdd(&total, cnt);
+    __syncthreads();
+    if (threadIdx.x == 0) terms[blockIdx.x] = total;
+}
+
+cudaError_t launch_ks_terms(const tfheb_params &p, int count, const int32_t *in, int in_stride, int32_t *terms,
+                            cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    ks_terms_kernel<<<count, 256, 0, s>>>(reinterpret_cast<const uint32_t *>(in), in_stride, p.k * p.N, p.ks_t,
+                                          p.ks_basebit, terms);
     return cudaGetLastError();
 }
 
