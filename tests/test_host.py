@@ -151,3 +151,31 @@ def test_blind_rotation_defaults_listed_first():
         G, D = tb.api.br_variants(N, prec)
         assert len(G) >= 2 and (int(G[0]), int(D[0])) == gd
         assert (G >= 1).all() and (D >= 3).all()
+
+
+def test_key_without_keyswitching_key_serves_rotations_only(tmp_path):
+    # a cloud key imported with a null keyswitching key (what the drop-in builds from caller-made
+    # TGSW samples): importing works, saving it in the reference's format is refused
+    p = tb.make_params(8, 1024, 1, 3, 7, 8, 2)
+    bsk = np.zeros((p.n, (p.k + 1) * p.l, p.k + 1, p.N), np.int32)
+    L = tb.api.lib()
+    h = ctypes.c_void_p()
+    assert L.tfheb_cloud_key_import(ctypes.byref(p), bsk.ctypes.data_as(ctypes.c_void_p), None, ctypes.byref(h)) == 0
+    try:
+        path = str(tmp_path / "ck.key")
+        assert L.tfheb_cloud_key_save(h, path.encode()) == 1
+        assert b"keyswitching key" in L.tfheb_last_error()
+    finally:
+        L.tfheb_cloud_key_free(h)
+
+
+def test_fft_plans_listed_per_variant():
+    # plan 0: one transform per thread; plan 1: two per thread on packed f32x2 with the spectra in
+    # tensor memory (split-FP32 only)
+    for N, prec in ((1024, tb.SPLIT_FP32), (2048, tb.SPLIT_FP32), (1024, tb.FP64), (2048, tb.FP64)):
+        p = tb.default_params() if N == 1024 else tb.large_params()
+        sk, ck = tb.keygen(tb.make_params(8, N, 1, 3, p.Bgbit, 8, 2), seed=1)
+        G, D = ck.br_variants(prec)
+        plans = ck.br_plans(prec)
+        assert len(plans) == len(G)
+        assert set(plans.tolist()) == ({0, 1} if prec == tb.SPLIT_FP32 else {0})

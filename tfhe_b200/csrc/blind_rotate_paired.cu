@@ -77,7 +77,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 
 // ---- shared memory and TMEM budget ---------------------------------------------------------------
 
-template <int N, int L, int G, int D, int XB>
+template <int N, int L, int G, int D, int XB, bool PW = true>
 struct PairLayout {
     static constexpr int M = N / 2, NT = M / kR, KP1 = 2, KPL = KP1 * L;
     static constexpr uint32_t half = (uint32_t)M * 16;  // one output's slots of one key row
@@ -90,7 +90,7 @@ struct PairLayout {
     static constexpr size_t team_xbuf = 16 * (size_t)Exch<double, M>::slots;
     static constexpr size_t team_bytes = team_acc + XB * team_xbuf;
     static constexpr size_t bytes = teams + G * team_bytes;
-    static constexpr int threads = G * NT + 32;
+    static constexpr int threads = G * NT + (PW ? 32 : 0);
     // TMEM: KPL spectra of 16 words per thread; warps of one lane quadrant take column slots in turn
     static constexpr int warps = G * NT / 32;
     static constexpr int cols_per_warp = KPL * 16;
@@ -103,9 +103,13 @@ struct PairLayout {
     static_assert(half % 16 == 0, "bulk copies need 16-byte sizes");
 };
 
-template <int N, int L, int G, int D, int XB>
-__global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_paired_kernel(const BrArgs args) {
-    using Lay = PairLayout<N, L, G, D, XB>;
+// PW: a key-streaming warp issues the half-row copies.  Without it, thread 0 issues them, as in
+// blind_rotate_kernel: the first D at the start, then each one as soon as every team has released its
+// slot, tested after each of its own half rows and waited for only when thread 0 needs one not yet
+// issued.  That frees the producer warp's registers (N = 2048 with two teams: 8 warps, 255 registers).
+template <int N, int L, int G, int D, int XB, bool PW>
+__global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_paired_kernel(const BrArgs args) {
+    using Lay = PairLayout<N, L, G, D, XB, PW>;
     constexpr int M = N / 2, NT = M / kR, KP1 = 2, KPL = KP1 * L;
     using F2 = TeamFft2<M>;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -142,6 +146,18 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_paired_kerne
 
     // half rows in consumption order: per step, output v = 0 then 1, each over the digits d
     const int total_chunks = args.nsteps * KP1 * KPL;
+    auto issue_row = [&](int c) {
+        const int s = c % D;
+        const int step = c / (KP1 * KPL), rem = c - step * (KP1 * KPL);
+        const int v = rem / KPL, d = rem - v * KPL;
+        const size_t src = ((size_t)(step * KPL + d) * KP1 + v) * Lay::half;
+        mbar_arrive_expect_tx(full_bar(s), Lay::half);
+        bulk_copy_g2s(ring + (uint32_t)s * Lay::half, args.bsk + src, Lay::half, full_bar(s));
+    };
+    int issued = 0;  // !PW: half rows issued by thread 0
+    bool issuing = !PW && tid == 0 && !args.stall_producer;
+    if (issuing)
+        for (; issued < min(D, total_chunks); issued++) issue_row(issued);
 
     // ---------------- producer warp: stream the key half rows ----------------
     if (tid >= consumers) {
@@ -152,11 +168,7 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_paired_kerne
                     const int s = c % D;
                     if (c >= D && !wait_bounded(empty_bar(s), ((c / D) - 1) & 1, abort_flag, args.timeout_ns, args.err))
                         break;
-                    const int step = c / (KP1 * KPL), rem = c - step * (KP1 * KPL);
-                    const int v = rem / KPL, d = rem - v * KPL;
-                    const size_t src = ((size_t)(step * KPL + d) * KP1 + v) * Lay::half;
-                    mbar_arrive_expect_tx(full_bar(s), Lay::half);
-                    bulk_copy_g2s(ring + (uint32_t)s * Lay::half, args.bsk + src, Lay::half, full_bar(s));
+                    issue_row(c);
                     sent = c + 1;
                 }
             }
@@ -276,6 +288,17 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_paired_kerne
                 const int c = (step * KP1 + v) * KPL + d, s = c % D;
                 uint32_t f[16];
                 tmem_ld16(tmem_row + (uint32_t)(d * 16), f);
+                if constexpr (!PW) {
+                    // thread 0 issues every half row before anyone waits for it
+                    while (issuing && issued <= c && issued < total_chunks) {
+                        if (!wait_bounded(empty_bar(issued % D), ((issued / D) - 1) & 1, abort_flag, args.timeout_ns,
+                                          args.err)) {
+                            issuing = false;
+                            break;
+                        }
+                        issue_row(issued++);
+                    }
+                }
                 wait_bounded(full_bar(s), (c / D) & 1, abort_flag, args.timeout_ns, args.err);
                 // half row: [m][limb][t] x float4 {re(2m), re(2m+1), im(2m), im(2m+1)}
                 const float4 *kp = reinterpret_cast<const float4 *>(smem + Lay::ring + (size_t)s * Lay::half) + t;
@@ -288,6 +311,11 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_paired_kerne
                     cmac_pair(al[m], zp, nzi, kp[(2 * m + 1) * NT]);
                 }
                 mbar_arrive(empty_bar(s));
+                if constexpr (!PW) {
+                    while (issuing && issued < total_chunks &&
+                           mbar_test_wait(empty_bar(issued % D), ((issued / D) - 1) & 1))
+                        issue_row(issued++);
+                }
             }
             // (hi, lo) per slot for the paired inverse
             cpair x[kR];
@@ -310,6 +338,14 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_paired_kerne
 
     uint32_t *dst = reinterpret_cast<uint32_t *>(args.acc_out) + (size_t)boot * KP1 * N;
     for (int i = t; i < KP1 * N; i += NT) dst[i] = s_acc[i];
+    if constexpr (!PW) {
+        // after an abort, drain the copies still in flight before the CTA may exit (bounded waits)
+        if (tid == 0) {
+            volatile int32_t no_abort = 0;
+            for (int r = (issued > D ? issued - D : 0); r < issued; r++)
+                wait_bounded(full_bar(r % D), (r / D) & 1, &no_abort, args.timeout_ns, args.err);
+        }
+    }
 
     // every consumer's TMEM accesses are complete (each load waited; stores waited per step)
     tmem_fence_before_sync();
@@ -319,11 +355,11 @@ __global__ void __launch_bounds__(G *(N / 16) + 32, 1) blind_rotate_paired_kerne
     if (warp == 0) tmem_free(tmem_base, Lay::tmem_cols);
 }
 
-template <int N, int L, int G, int D, int XB>
+template <int N, int L, int G, int D, int XB, bool PW>
 cudaError_t launch_paired(const BrArgs &a, cudaStream_t s) {
-    using Lay = PairLayout<N, L, G, D, XB>;
+    using Lay = PairLayout<N, L, G, D, XB, PW>;
     if (!a.tables2) return cudaErrorInvalidValue;
-    auto kern = blind_rotate_paired_kernel<N, L, G, D, XB>;
+    auto kern = blind_rotate_paired_kernel<N, L, G, D, XB, PW>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::bytes);
     if (e != cudaSuccess) return e;
     const int grid = (a.boots + G - 1) / G;
@@ -331,12 +367,13 @@ cudaError_t launch_paired(const BrArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template cudaError_t launch_paired<1024, 3, 7, 8, 1>(const BrArgs &, cudaStream_t);
-template cudaError_t launch_paired<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
-template cudaError_t launch_paired<1024, 3, 7, 4, 2>(const BrArgs &, cudaStream_t);
-template cudaError_t launch_paired<1024, 3, 6, 6, 2>(const BrArgs &, cudaStream_t);
-template cudaError_t launch_paired<2048, 3, 2, 4, 2>(const BrArgs &, cudaStream_t);
-template cudaError_t launch_paired<2048, 3, 2, 6, 2>(const BrArgs &, cudaStream_t);
-template cudaError_t launch_paired<2048, 3, 3, 4, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<1024, 3, 7, 8, 1, true>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<1024, 3, 7, 12, 1, true>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<1024, 3, 7, 4, 2, true>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<1024, 3, 6, 6, 2, true>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<2048, 3, 2, 4, 2, false>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<2048, 3, 2, 6, 2, false>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<2048, 3, 2, 4, 2, true>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<2048, 3, 3, 4, 1, true>(const BrArgs &, cudaStream_t);
 
 }  // namespace tfheb

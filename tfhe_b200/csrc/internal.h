@@ -187,7 +187,7 @@ cudaError_t launch_extern_product(const tfheb_params &p, int precision, const De
                                   uint64_t timeout_ns);
 // blind_rotate_paired.cu: the split-FP32 variants with two transforms per thread (plan 1)
 struct BrArgs;
-template <int N, int L, int G, int D, int XB>
+template <int N, int L, int G, int D, int XB, bool PW>
 cudaError_t launch_paired(const BrArgs &a, cudaStream_t s);
 // keyswitch.cu: device key upload (both layouts) and the keyswitch of `count` extracted samples
 // (rows of in_stride int32) into rows of n+1 int32.

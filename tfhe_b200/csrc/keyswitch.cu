@@ -333,9 +333,13 @@ __global__ void __launch_bounds__(256, 1)
         }
         const int st_i = q % L::stages;
         const bool ok = wait_bounded(bars + 8 * st_i, (q / L::stages) & 1, abort_flag, timeout_ns, err);
+        // every lane reads the same word; the OR over the warp returns it as a value the compiler
+        // knows to be warp-uniform, so the digit arithmetic and the branches below can run on the
+        // uniform datapath without convergence barriers
         uint32_t abar[G];
 #pragma unroll
-        for (int s = 0; s < G; s++) abar[s] = s_a[(q & (kKsChunk - 1)) * L::sa_ld + warp * G + s];
+        for (int s = 0; s < G; s++)
+            abar[s] = __reduce_or_sync(0xffffffffu, s_a[(q & (kKsChunk - 1)) * L::sa_ld + warp * G + s]);
         const uint32_t *stage = ring + st_i * L::stage_words + 2 * lane;
 #pragma unroll 1
         for (int j = 0; j < kKsT; j++) {
