@@ -746,13 +746,15 @@ struct BrVariant {
     int plan = 0;  // 0: one transform per thread; 1: two per thread, spectra in TMEM (blind_rotate_paired.cu)
 };
 static const BrVariant kBrVariants[] = {
+    // the split default: two transforms per thread, spectra in TMEM, a 12-half-row key ring
+    // (33.15 ms per 4096 bootstraps against 36.24 ms for the plan-0 G = 7, D = 6 below)
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired<1024, 3, 7, 12, 1, true>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 6, true, launch_g<float, 1024, 3, true, 7, 6>},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 4, true, launch_g<float, 1024, 3, true, 7, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 5, 4, true, launch_g<float, 1024, 3, true, 5, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 4, 4, true, launch_g<float, 1024, 3, true, 4, 4>},
     // plan 1: D counts half rows (8 KB) here; single or double exchange buffers per team
     {1024, 3, TFHEB_SPLIT_FP32, 7, 8, true, launch_paired<1024, 3, 7, 8, 1, true>, 1},
-    {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired<1024, 3, 7, 12, 1, true>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 4, true, launch_paired<1024, 3, 7, 4, 2, true>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 6, 6, true, launch_paired<1024, 3, 6, 6, 2, true>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 3, 4, false, launch_g<float, 1024, 3, true, 3, 4>},
@@ -767,15 +769,16 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_FP64, 2, 4, true, launch_g<double, 1024, 3, false, 2, 4>},
     {1024, 3, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 3, false, 1, 4>},
     {1024, 3, TFHEB_FP64, 1, 6, false, launch_wide<double, 1024, 3, false, 6, 1>},
+    // the split default at N = 2048: two transforms per thread, three teams (56.8 ms per 2048
+    // bootstraps against 62.6 ms for the plan-0 G = 2 below)
+    {2048, 3, TFHEB_SPLIT_FP32, 3, 4, true, launch_paired<2048, 3, 3, 4, 1, true>, 1},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_g<float, 2048, 3, true, 2, 4, false>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_g<float, 2048, 3, true, 2, 4>},
     {2048, 3, TFHEB_SPLIT_FP32, 3, 3, true, launch_g<float, 2048, 3, true, 3, 3>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 3, true, launch_g<float, 2048, 3, true, 2, 3>},
     {2048, 3, TFHEB_SPLIT_FP32, 1, 3, false, launch_g<float, 2048, 3, true, 1, 3>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_paired<2048, 3, 2, 4, 2, false>, 1},
-    {2048, 3, TFHEB_SPLIT_FP32, 2, 6, true, launch_paired<2048, 3, 2, 6, 2, false>, 1},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_paired<2048, 3, 2, 4, 2, true>, 1},
-    {2048, 3, TFHEB_SPLIT_FP32, 3, 4, true, launch_paired<2048, 3, 3, 4, 1, true>, 1},
     {2048, 3, TFHEB_FP64, 2, 3, true, launch_g<double, 2048, 3, false, 2, 3, false>},
     {2048, 3, TFHEB_FP64, 2, 3, true, launch_g<double, 2048, 3, false, 2, 3>},
     {2048, 3, TFHEB_FP64, 1, 4, true, launch_g<double, 2048, 3, false, 1, 4>},

@@ -60,17 +60,32 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// 16 consecutive columns of this thread's lane, waited for in the same statement so that no use of
-// the registers can be scheduled before the data has arrived
+// 16 consecutive columns of this thread's lane.  The load completes asynchronously: tmem_wait_ld16
+// takes the same registers as in-out operands, so no use of them can be scheduled before the wait.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];\n\t"
-        "tcgen05.wait::ld.sync.aligned;"
+        "%15}, [%16];"
         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
           "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
         : "r"(taddr)
         : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld16(uint32_t (&v)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                   "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
+                   "+r"(v[15])
+                 :
+                 : "memory");
+}
+
+// Two digits as floats in one packed pair: the bits of 1.5*2^23 + d of each (digit mask and OR in one
+// logic op), then one packed subtraction of the bias.  sub_bias_neg gives -(x - bias) as bias - x, the
+// same value (round to nearest is symmetric; only the sign of a zero may differ, which no later
+// operation can turn into a different rounded result).
+__device__ __forceinline__ float2 digit_pair(uint32_t a, uint32_t b) {
+    return make_float2(__int_as_float(0x4B400000u | a), __int_as_float(0x4B400000u | b));
 }
 
 }  // namespace
@@ -245,14 +260,13 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
             const int u0 = d0 / L, q0 = d0 % L, u1 = (d0 + 1) / L, q1 = (d0 + 1) % L;
             const int sh0 = 32 - (q0 + 1) * Bgbit, sh1 = 32 - (q1 + 1) * Bgbit;
             cpair z[kR];
+            const float2 bias2 = make_float2(digit_bias, digit_bias);
 #pragma unroll
             for (int r = 0; r < kR; r++) {
                 // a_j - i a_{j+M} of each digit polynomial; the twist is folded into the FFT
-                const float a0 = biased_to_float((xr[u0][r] >> sh0) & maskBg, digit_bias);
-                const float a1 = biased_to_float((xr[u0][kR + r] >> sh0) & maskBg, digit_bias);
-                const float b0 = biased_to_float((xr[u1][r] >> sh1) & maskBg, digit_bias);
-                const float b1 = biased_to_float((xr[u1][kR + r] >> sh1) & maskBg, digit_bias);
-                z[r] = {make_float2(a0, b0), make_float2(-a1, -b1)};
+                const float2 lo = digit_pair((xr[u0][r] >> sh0) & maskBg, (xr[u1][r] >> sh1) & maskBg);
+                const float2 hi = digit_pair((xr[u0][kR + r] >> sh0) & maskBg, (xr[u1][kR + r] >> sh1) & maskBg);
+                z[r] = {sub2(lo, bias2), sub2(bias2, hi)};
             }
             F2::forward(z, xp, s_tw2, t, bar_id);
             // spectrum words in multiply-accumulate order: per register pair m, re(2m), re(2m+1),
@@ -283,11 +297,15 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
                 ah[m] = {{0.f, 0.f}, {0.f, 0.f}};
                 al[m] = {{0.f, 0.f}, {0.f, 0.f}};
             }
-#pragma unroll 1
+            // digit spectra from TMEM, the next one loading while this one is multiplied
+            uint32_t fb[2][16];
+            tmem_ld16(tmem_row, fb[0]);
+            tmem_wait_ld16(fb[0]);
+#pragma unroll
             for (int d = 0; d < KPL; d++) {
                 const int c = (step * KP1 + v) * KPL + d, s = c % D;
-                uint32_t f[16];
-                tmem_ld16(tmem_row + (uint32_t)(d * 16), f);
+                uint32_t(&f)[16] = fb[d & 1];
+                if (d + 1 < KPL) tmem_ld16(tmem_row + (uint32_t)((d + 1) * 16), fb[(d + 1) & 1]);
                 if constexpr (!PW) {
                     // thread 0 issues every half row before anyone waits for it
                     while (issuing && issued <= c && issued < total_chunks) {
@@ -316,6 +334,7 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
                            mbar_test_wait(empty_bar(issued % D), ((issued / D) - 1) & 1))
                         issue_row(issued++);
                 }
+                if (d + 1 < KPL) tmem_wait_ld16(fb[(d + 1) & 1]);
             }
             // (hi, lo) per slot for the paired inverse
             cpair x[kR];
@@ -372,7 +391,6 @@ template cudaError_t launch_paired<1024, 3, 7, 12, 1, true>(const BrArgs &, cuda
 template cudaError_t launch_paired<1024, 3, 7, 4, 2, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<1024, 3, 6, 6, 2, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 2, 4, 2, false>(const BrArgs &, cudaStream_t);
-template cudaError_t launch_paired<2048, 3, 2, 6, 2, false>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 2, 4, 2, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 3, 4, 1, true>(const BrArgs &, cudaStream_t);
 
