@@ -421,13 +421,15 @@ void run_batch(int32_t gate, LweSample *res, const LweSample *a, const LweSample
 class Staged {
   public:
     Staged(StagingArea &area, tfheb_cloud_key *ck, size_t words) : a_(area), lock_(area.mu), ck_(ck) {
+        // the copies below run on the key's stream from whatever host thread calls: make its device
+        // current here, not only when the buffers grow
+        if (cudaSetDevice(ck->ck.device) != cudaSuccess) die("selecting the key's GPU");
         if (words > a_.cap) {
             if (a_.h) cudaFreeHost(a_.h);
             if (a_.d) cudaFree(a_.d);
             a_.h = a_.d = nullptr;
             a_.cap = 0;
-            if (cudaSetDevice(ck->ck.device) != cudaSuccess || cudaMallocHost((void **)&a_.h, words * 4) != cudaSuccess ||
-                cudaMalloc((void **)&a_.d, words * 4) != cudaSuccess)
+            if (cudaMallocHost((void **)&a_.h, words * 4) != cudaSuccess || cudaMalloc((void **)&a_.d, words * 4) != cudaSuccess)
                 die("staging buffers");
             a_.cap = words;
         }
