@@ -198,7 +198,7 @@ def run_extra_workload(args):
         rng = np.random.default_rng(B)
         x = torch.from_numpy(rng.integers(-2**31, 2**31, (B, p.k * p.N + 1), dtype=np.int64).astype(np.int32)).cuda()
         ref_out, times = None, {}
-        for which, name in ((1, "per_sample"), (2, "tiled"), (3, "regkey")):
+        for which, name in ((1, "per_sample"), (2, "tiled"), (3, "regkey"), (4, "tensor_core")):
             ck.set_keyswitch_kernel(which)
             dout = torch.zeros((B, p.n + 1), dtype=torch.int32, device="cuda")
             for _ in range(args.warmup):

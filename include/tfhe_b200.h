@@ -298,10 +298,11 @@ tfheb_status tfheb_set_br_variant(tfheb_cloud_key *ck, int32_t precision, int32_
 tfheb_status tfheb_autotune(tfheb_cloud_key *ck, int32_t precision, int32_t boots, double *ms, int32_t cap);
 
 /* Keyswitch kernel of a key: 0 = default, 1 = one CTA per sample, 2 = tiled (key rows shared
- * through shared memory), 3 = register-key (key rows held in registers across samples); 2 and 3
- * need ks_t = 8 and basebit = 2 (TFHEB_ERR_UNSUPPORTED otherwise), which the default also uses
- * when it can.  Both give the reference's lweKeySwitch result bit for bit; the choice is a
- * performance knob.  No reference counterpart. */
+ * through shared memory), 3 = register-key (key rows held in registers across samples),
+ * 4 = tensor-core (the digit selection as an int8 one-hot product with the key's byte planes on
+ * tcgen05.mma); 2 to 4 need ks_t = 8 and basebit = 2 (TFHEB_ERR_UNSUPPORTED otherwise), which the
+ * default also uses when it can.  All give the reference's lweKeySwitch result bit for bit; the
+ * choice is a performance knob.  No reference counterpart. */
 tfheb_status tfheb_set_keyswitch_kernel(tfheb_cloud_key *ck, int32_t which);
 
 /* Weight exponent S of the high limb the split-FP32 key uses by default for a parameter set. */

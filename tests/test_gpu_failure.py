@@ -32,7 +32,8 @@ def test_stalled_key_stream_reports_timeout_and_context_survives(precision):
     assert (bits == g["out_bits"][sel]).all()
 
 
-@pytest.mark.parametrize("kernel", [2, 3])  # tiled, register-key: both stream key rows through a ring
+# tiled, register-key, tensor-core: all stream key rows through a ring
+@pytest.mark.parametrize("kernel", [2, 3, 4])
 def test_stalled_keyswitch_ring_reports_timeout_and_context_survives(kernel):
     torch = pytest.importorskip("torch")
     g = np.load(os.path.join(GOLDEN, "gates_small.npz"))

@@ -82,7 +82,7 @@ def test_keyswitch_other_shape_bit_exact_vs_reference_golden():
     out = torch.zeros((len(x), p.n + 1), dtype=torch.int32, device="cuda")
     ck.keyswitch_device(dev(x), out, len(x))
     assert (host(out) == g["ks_outputs"]).all()
-    for which in (2, 3):
+    for which in (2, 3, 4):
         with pytest.raises(tb.api.TfhebError, match="no tiled keyswitch"):
             ck.set_keyswitch_kernel(which)
 
@@ -124,7 +124,8 @@ def _keyswitch_with(ck, p, x, which, fill):
 
 
 # batch sizes: 1 and 63 split the coefficient range over CTAs (atomic combination), 64/65/300 give
-# full and ragged 64-sample tiles, 2100 more tiles than one wave of CTAs
+# full and ragged 64-sample tiles (256-sample tiles of the tensor-core kernel: 300 and 2100 end
+# ragged), 2100 more tiles than one wave of CTAs
 @pytest.mark.parametrize("count", [1, 63, 64, 65, 300, 2100])
 def test_keyswitch_kernels_agree_bit_for_bit(oracle, default_keys, count):
     p, sk, ck, bsk, ksk = default_keys
@@ -134,8 +135,10 @@ def test_keyswitch_kernels_agree_bit_for_bit(oracle, default_keys, count):
     per_sample = _keyswitch_with(ck, p, x, 1, 0)
     tiled = _keyswitch_with(ck, p, x, 2, -7)  # garbage in the output rows must not leak through
     regkey = _keyswitch_with(ck, p, x, 3, 13)
+    tensor_core = _keyswitch_with(ck, p, x, 4, 99)
     assert (tiled == per_sample).all()
     assert (regkey == per_sample).all()
+    assert (tensor_core == per_sample).all()
     pick = sorted({0, count - 1, count // 2})
     assert (tiled[pick] == oracle.keyswitch(pdict(p), ksk, x[pick])).all()
 
@@ -147,6 +150,7 @@ def test_keyswitch_tiled_large_params_bit_exact(oracle, large_keys):
     tiled = _keyswitch_with(ck, p, x, 2, 5)
     assert (tiled == _keyswitch_with(ck, p, x, 1, 0)).all()
     assert (tiled == _keyswitch_with(ck, p, x, 3, -3)).all()
+    assert (tiled == _keyswitch_with(ck, p, x, 4, 17)).all()
     assert (tiled[[0, 129]] == oracle.keyswitch(pdict(p), ksk, x[[0, 129]])).all()
 
 

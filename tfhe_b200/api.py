@@ -285,7 +285,8 @@ class CloudKey:
         _check(lib().tfheb_set_br_variant(self.h, precision, variant), "tfheb_set_br_variant")
 
     def set_keyswitch_kernel(self, which):
-        """0 = default, 1 = one CTA per sample, 2 = tiled, 3 = register-key (bit-identical results)."""
+        """0 = default, 1 = one CTA per sample, 2 = tiled, 3 = register-key, 4 = tensor-core
+        (bit-identical results)."""
         _check(lib().tfheb_set_keyswitch_kernel(self.h, which), "tfheb_set_keyswitch_kernel")
 
     def set_wait_timeout(self, seconds):

@@ -866,7 +866,7 @@ tfheb_status tfheb_set_br_variant(tfheb_cloud_key *c, int32_t precision, int32_t
 }
 
 tfheb_status tfheb_set_keyswitch_kernel(tfheb_cloud_key *c, int32_t which) {
-    if (!c || which < 0 || which > 3) return TFHEB_ERR_INVALID;
+    if (!c || which < 0 || which > 4) return TFHEB_ERR_INVALID;
     std::lock_guard<std::mutex> lock(c->mu);
     const tfheb_params &p = c->ck.p;
     if (which >= 2 && !(p.ks_t == 8 && p.ks_basebit == 2)) {

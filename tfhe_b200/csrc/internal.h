@@ -53,6 +53,8 @@ struct DeviceKsk {
     int rk_c = 0;              // output columns per lane of the register-key kernel (0: unavailable)
     int rk_slices = 0;         // column blocks of 32 * rk_c columns covering n+1
     int rk_slots = 0;          // resident CTAs of the register-key kernel on the device
+    uint8_t *mma = nullptr;    // tensor-core kernel: [group][kN][8 KB], the B operand's shared-memory image
+    int mma_groups = 0;        // 64-column groups covering n+1 (0: tensor-core kernel unavailable)
 };
 
 // What a reference parameter file carries beyond tfheb_params: the LWE and TLWE alpha_max
@@ -84,7 +86,7 @@ struct CloudKey {
     int device = -1;
     DeviceBsk dbsk[2];              // [TFHEB_FP64], [TFHEB_SPLIT_FP32]
     DeviceKsk dksk;
-    int ks_kernel = 0;              // 0 = default, 1 = per-sample, 2 = tiled, 3 = register-key
+    int ks_kernel = 0;              // 0 = default, 1 = per-sample, 2 = tiled, 3 = register-key, 4 = tensor-core
     cudaStream_t stream = nullptr;
     // scratch (grown on demand)
     int32_t *d_bara = nullptr;
@@ -192,6 +194,9 @@ cudaError_t launch_paired(const BrArgs &a, cudaStream_t s);
 // keyswitch.cu: device key upload (both layouts) and the keyswitch of `count` extracted samples
 // (rows of in_stride int32) into rows of n+1 int32.
 cudaError_t upload_keyswitch_key(CloudKey &ck);
+cudaError_t upload_keyswitch_key_mma(CloudKey &ck);  // keyswitch_mma.cu
+cudaError_t launch_keyswitch_mma(const CloudKey &ck, int count, const int32_t *in, int in_stride, int32_t *out,
+                                 cudaStream_t s);
 void free_keyswitch_key(DeviceKsk &d);
 cudaError_t launch_keyswitch(const CloudKey &ck, int count, const int32_t *in, int in_stride, int32_t *out,
                              cudaStream_t s);

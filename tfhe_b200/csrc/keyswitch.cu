@@ -6,7 +6,8 @@
 // with digit_j the j-th basebit-bit digit from the top.  All arithmetic is mod 2^32, so any order of
 // the additions gives the reference's result bit for bit.
 //
-// Three kernels:
+// Three CUDA-core kernels here, and the tensor-core kernel of keyswitch_mma.cu (the default wherever
+// t = 8 and basebit = 2; the three below remain as cross-checks and for other digit shapes):
 //   keyswitch_gate_kernel   one CTA per sample, each thread 4 output columns; the selected key rows are
 //                           gathered from L2 per sample (15.5 MB of rows per sample at n = 630).  Used
 //                           for parameter sets without a tiled instantiation, or on request.
@@ -17,10 +18,10 @@
 //                           at most 4 distinct rows (digit 0 reads a zero row) and every 16-byte load
 //                           is a broadcast.  L2->SM key traffic drops from 15.5 MB per sample to 15.5 MB
 //                           per 64 samples.  Small batches split the i range over CTAs and combine the
-//                           partial sums with atomic adds (mod 2^32, exact).  Default below 256 samples.
+//                           partial sums with atomic adds (mod 2^32, exact).
 //   keyswitch_regkey_kernel lane = column pair, key rows of one (i, j) held in registers and applied to
 //                           7 samples per warp through a warp-uniform digit branch; each loaded key
-//                           word serves 7 subtractions.  Default from 256 samples.
+//                           word serves 7 subtractions.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -469,7 +470,6 @@ cudaError_t tiled_slots(int device, int *slots) {
     return cudaSuccess;
 }
 
-constexpr int kRegKeyMinCount = 256;  // default kernel switch-over (samples per call)
 
 // register-key instantiations: columns per lane C and samples per warp G
 constexpr int kRkC[] = {10, 14};
@@ -586,13 +586,14 @@ cudaError_t upload_keyswitch_key(CloudKey &ck) {
         d.rk_c = c;
         d.rk_slices = slices;
     }
-    return cudaSuccess;
+    return upload_keyswitch_key_mma(ck);
 }
 
 void free_keyswitch_key(DeviceKsk &d) {
     if (d.rows) cudaFree(d.rows);
     if (d.tiles) cudaFree(d.tiles);
     if (d.rk) cudaFree(d.rk);
+    if (d.mma) cudaFree(d.mma);
     d = DeviceKsk{};
 }
 
@@ -600,10 +601,13 @@ cudaError_t launch_keyswitch(const CloudKey &ck, int count, const int32_t *in, i
                              cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
     const tfheb_params &p = ck.p;
-    // default: the register-key kernel from kRegKeyMinCount samples (measured 2.00 vs 2.88 ms per
-    // 4096 and 0.63 vs 0.74 ms per 1036 samples against the tiled kernel), the tiled kernel below
-    // (0.047 vs 0.086 ms for one sample: more CTAs share a small batch)
-    const bool regkey = ck.ks_kernel == 3 || (ck.ks_kernel == 0 && count >= kRegKeyMinCount);
+    // default: the tensor-core kernel wherever it is built (t = 8, basebit = 2), at every batch size
+    // (measured per 4096 / 1036 / 256 / 1 samples: 0.305 / 0.114 / 0.044 / 0.035 ms, against 1.82 /
+    // 0.578 / 0.225 / 0.077 ms for the register-key and 2.89 / 0.738 / 0.196 / 0.049 ms for the
+    // tiled kernel); otherwise the one-CTA-per-sample kernel
+    if ((ck.ks_kernel == 4 || ck.ks_kernel == 0) && ck.dksk.mma_groups != 0)
+        return launch_keyswitch_mma(ck, count, in, in_stride, out, s);
+    const bool regkey = ck.ks_kernel == 3;
     if (regkey && ck.dksk.rk_c != 0) {
         switch (ck.dksk.rk_c) {
             case 10: return launch_regkey<10, 7>(ck, count, in, in_stride, out, s);
