@@ -769,8 +769,10 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_FP64, 2, 4, true, launch_g<double, 1024, 3, false, 2, 4>},
     {1024, 3, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 3, false, 1, 4>},
     {1024, 3, TFHEB_FP64, 1, 6, false, launch_wide<double, 1024, 3, false, 6, 1>},
-    // the split default at N = 2048: two transforms per thread, three teams (56.8 ms per 2048
-    // bootstraps against 62.6 ms for the plan-0 G = 2 below)
+    // the split default at N = 2048: two transforms per thread, three teams, a 6-deep ring of 16 KB
+    // half rows (54.0 ms per 2048 bootstraps against 56.5 ms 4 deep and 62.6 ms for the plan-0 G = 2
+    // below)
+    {2048, 3, TFHEB_SPLIT_FP32, 3, 6, true, launch_paired<2048, 3, 3, 6, 1, true>, 1},
     {2048, 3, TFHEB_SPLIT_FP32, 3, 4, true, launch_paired<2048, 3, 3, 4, 1, true>, 1},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_g<float, 2048, 3, true, 2, 4, false>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_g<float, 2048, 3, true, 2, 4>},

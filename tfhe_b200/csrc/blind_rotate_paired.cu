@@ -345,5 +345,6 @@ template cudaError_t launch_paired<1024, 3, 6, 6, 2, true>(const BrArgs &, cudaS
 template cudaError_t launch_paired<2048, 3, 2, 4, 2, false>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 2, 4, 2, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 3, 4, 1, true>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired<2048, 3, 3, 6, 1, true>(const BrArgs &, cudaStream_t);
 
 }  // namespace tfheb
