@@ -145,7 +145,8 @@ def test_bench_script_parses_and_lists_its_workloads():
 def test_blind_rotation_defaults_listed_first():
     # the first candidate of each parameter set is the default until tfheb_autotune measures
     # otherwise: split G=7 with a 12-half-row ring (two transforms per thread) and FP64 G=4 D=5 at
-    # N=1024 (l=3); at N=2048 split G=3 with a 6-deep ring (two transforms per thread), FP64 G=2
+    # N=1024 (l=3); at N=2048 split G=3 with a 6-deep ring (two transforms per thread, the rotated
+    # words parked in TMEM), FP64 G=2
     want = {(1024, tb.SPLIT_FP32): (7, 12), (1024, tb.FP64): (4, 5),
             (2048, tb.SPLIT_FP32): (3, 6), (2048, tb.FP64): (2, 3)}
     for (N, prec), gd in want.items():

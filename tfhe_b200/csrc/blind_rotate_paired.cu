@@ -16,6 +16,9 @@
 //   * The key ring holds half rows, one output polynomial's slots of one digit row (8 KB at N =
 //     1024), streamed in the order of the multiply-accumulate: per step, output 0 over the digits,
 //     then output 1.
+//   * XT variants also park the step's rotated words (32 per thread) in TMEM between the rotation
+//     and the digit extraction of each transform pair, so that they hold no registers across the
+//     forward transforms.
 // Every mbarrier wait is bounded as in blind_rotate_kernel.  Warp 0 allocates the TMEM columns at
 // the start and frees them after every consumer thread has passed a final barrier, on every path
 // (a wait that runs out only makes the remaining waits return at once).
@@ -44,7 +47,7 @@ __device__ __forceinline__ float2 digit_pair(uint32_t a, uint32_t b) {
 
 // ---- shared memory and TMEM budget ---------------------------------------------------------------
 
-template <int N, int L, int G, int D, int XB, bool PW = true>
+template <int N, int L, int G, int D, int XB, bool PW = true, bool XT = false>
 struct PairLayout {
     static constexpr int M = N / 2, NT = M / kR, KP1 = 2, KPL = KP1 * L;
     static constexpr uint32_t half = (uint32_t)M * 16;  // one output's slots of one key row
@@ -61,7 +64,10 @@ struct PairLayout {
     // TMEM: KPL spectra of 16 words per thread; warps of one lane quadrant take column slots in turn
     static constexpr int warps = G * NT / 32;
     static constexpr int cols_per_warp = KPL * 16;
-    static constexpr int cols_needed = (warps + 3) / 4 * cols_per_warp;
+    static constexpr int spectra_cols = (warps + 3) / 4 * cols_per_warp;
+    // XT: the step's rotated words (32 per thread) wait in TMEM during the forward transforms
+    static constexpr int xr_col = spectra_cols;
+    static constexpr int cols_needed = spectra_cols + (XT ? (warps + 3) / 4 * 32 : 0);
     static constexpr int tmem_cols = cols_needed <= 32 ? 32 : cols_needed <= 64 ? 64 : cols_needed <= 128 ? 128
                                    : cols_needed <= 256 ? 256 : 512;
     static_assert(cols_needed <= 512, "TMEM columns of the variant");
@@ -74,9 +80,9 @@ struct PairLayout {
 // blind_rotate_kernel: the first D at the start, then each one as soon as every team has released its
 // slot, tested after each of its own half rows and waited for only when thread 0 needs one not yet
 // issued.  That frees the producer warp's registers (N = 2048 with two teams: 8 warps, 255 registers).
-template <int N, int L, int G, int D, int XB, bool PW>
+template <int N, int L, int G, int D, int XB, bool PW, bool XT>
 __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_paired_kernel(const BrArgs args) {
-    using Lay = PairLayout<N, L, G, D, XB, PW>;
+    using Lay = PairLayout<N, L, G, D, XB, PW, XT>;
     constexpr int M = N / 2, NT = M / kR, KP1 = 2, KPL = KP1 * L;
     using F2 = TeamFft2<M>;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -161,6 +167,7 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
     const float4 *s_tw2 = reinterpret_cast<const float4 *>(smem + Lay::tables);
     // this thread's TMEM row: lane quadrant of its warp, the warp's column slot within the quadrant
     const uint32_t tmem_row = tmem_base + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((warp >> 2) * Lay::cols_per_warp);
+    const uint32_t tmem_xr = tmem_base + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(Lay::xr_col + (warp >> 2) * 32);
 
     const int32_t *my_bara = args.bara + (size_t)boot * args.bara_stride;
     if (args.acc_in) {
@@ -206,18 +213,31 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
                 xr[u][r] = rot_minus_one<N>(s_acc + u * N, j, ai) + offset;
                 xr[u][kR + r] = rot_minus_one<N>(s_acc + u * N, j + M, ai) + offset;
             }
+        if constexpr (XT) {
+            tmem_st32(tmem_xr, reinterpret_cast<uint32_t(&)[32]>(xr));
+            tmem_wait_st();
+        }
         // 2. digits two at a time in chain order d = u*L + q, forward transforms, spectra to TMEM
 #pragma unroll
         for (int d0 = 0; d0 < KPL; d0 += 2) {
             const int u0 = d0 / L, q0 = d0 % L, u1 = (d0 + 1) / L, q1 = (d0 + 1) % L;
             const int sh0 = 32 - (q0 + 1) * Bgbit, sh1 = 32 - (q1 + 1) * Bgbit;
+            uint32_t xw[KP1][2 * kR];  // XT: the words of the polynomials this pair reads, from TMEM
+            if constexpr (XT) {
+                tmem_ld16(tmem_xr + (uint32_t)(16 * u0), xw[u0]);
+                if (u1 != u0) tmem_ld16(tmem_xr + (uint32_t)(16 * u1), xw[u1]);
+                tmem_wait_ld16(xw[u0]);
+                if (u1 != u0) tmem_wait_ld16(xw[u1]);
+            }
+            const uint32_t(&xa)[2 * kR] = XT ? xw[u0] : xr[u0];
+            const uint32_t(&xb)[2 * kR] = XT ? xw[u1] : xr[u1];
             cpair z[kR];
             const float2 bias2 = make_float2(digit_bias, digit_bias);
 #pragma unroll
             for (int r = 0; r < kR; r++) {
                 // a_j - i a_{j+M} of each digit polynomial; the twist is folded into the FFT
-                const float2 lo = digit_pair((xr[u0][r] >> sh0) & maskBg, (xr[u1][r] >> sh1) & maskBg);
-                const float2 hi = digit_pair((xr[u0][kR + r] >> sh0) & maskBg, (xr[u1][kR + r] >> sh1) & maskBg);
+                const float2 lo = digit_pair((xa[r] >> sh0) & maskBg, (xb[r] >> sh1) & maskBg);
+                const float2 hi = digit_pair((xa[kR + r] >> sh0) & maskBg, (xb[kR + r] >> sh1) & maskBg);
                 z[r] = {sub2(lo, bias2), sub2(bias2, hi)};
             }
             F2::forward(z, xp, s_tw2, t, bar_id);
@@ -326,16 +346,25 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
     if (warp == 0) tmem_free(tmem_base, Lay::tmem_cols);
 }
 
-template <int N, int L, int G, int D, int XB, bool PW>
-cudaError_t launch_paired(const BrArgs &a, cudaStream_t s) {
-    using Lay = PairLayout<N, L, G, D, XB, PW>;
+template <int N, int L, int G, int D, int XB, bool PW, bool XT>
+static cudaError_t launch_paired_impl(const BrArgs &a, cudaStream_t s) {
+    using Lay = PairLayout<N, L, G, D, XB, PW, XT>;
     if (!a.tables2) return cudaErrorInvalidValue;
-    auto kern = blind_rotate_paired_kernel<N, L, G, D, XB, PW>;
+    auto kern = blind_rotate_paired_kernel<N, L, G, D, XB, PW, XT>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::bytes);
     if (e != cudaSuccess) return e;
     const int grid = (a.boots + G - 1) / G;
     kern<<<grid, Lay::threads, Lay::bytes, s>>>(a);
     return cudaGetLastError();
+}
+
+template <int N, int L, int G, int D, int XB, bool PW>
+cudaError_t launch_paired(const BrArgs &a, cudaStream_t s) {
+    return launch_paired_impl<N, L, G, D, XB, PW, false>(a, s);
+}
+template <int N, int L, int G, int D, int XB>
+cudaError_t launch_paired_xt(const BrArgs &a, cudaStream_t s) {
+    return launch_paired_impl<N, L, G, D, XB, true, true>(a, s);
 }
 
 template cudaError_t launch_paired<1024, 3, 7, 8, 1, true>(const BrArgs &, cudaStream_t);
@@ -345,6 +374,8 @@ template cudaError_t launch_paired<1024, 3, 6, 6, 2, true>(const BrArgs &, cudaS
 template cudaError_t launch_paired<2048, 3, 2, 4, 2, false>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 2, 4, 2, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 3, 4, 1, true>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_xt<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_xt<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 3, 6, 1, true>(const BrArgs &, cudaStream_t);
 
 }  // namespace tfheb
