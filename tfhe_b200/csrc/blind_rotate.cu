@@ -746,8 +746,11 @@ struct BrVariant {
     int plan = 0;  // 0: one transform per thread; 1: two per thread, spectra in TMEM (blind_rotate_paired.cu)
 };
 static const BrVariant kBrVariants[] = {
-    // the split default: two transforms per thread, spectra in TMEM, a 12-half-row key ring
-    // (33.15 ms per 4096 bootstraps against 36.24 ms for the plan-0 G = 7, D = 6 below)
+    // the split default: two transforms per thread, spectra in TMEM, a 12-half-row key ring, the
+    // step's rotated words parked in TMEM and the first two digit pairs' forward transforms
+    // interleaved (31.83 ms per 4096 bootstraps, no spills; 32.24 ms for the same without the last
+    // two, 36.24 ms for the plan-0 G = 7, D = 6 below)
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_il<1024, 3, 7, 12, 1>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired<1024, 3, 7, 12, 1, true>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 6, true, launch_g<float, 1024, 3, true, 7, 6>},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 4, true, launch_g<float, 1024, 3, true, 7, 4>},
@@ -757,7 +760,7 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_SPLIT_FP32, 7, 8, true, launch_paired<1024, 3, 7, 8, 1, true>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 4, true, launch_paired<1024, 3, 7, 4, 2, true>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 6, 6, true, launch_paired<1024, 3, 6, 6, 2, true>, 1},
-    // the rotated words in TMEM: no spills at 128 registers, 32.4 ms against 32.2 for the default
+    // the rotated words in TMEM without the interleave: 32.4 ms
     {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_xt<1024, 3, 7, 12, 1>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 3, 4, false, launch_g<float, 1024, 3, true, 3, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 2, 4, false, launch_g<float, 1024, 3, true, 2, 4>},
@@ -772,9 +775,10 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 3, false, 1, 4>},
     {1024, 3, TFHEB_FP64, 1, 6, false, launch_wide<double, 1024, 3, false, 6, 1>},
     // the split default at N = 2048: two transforms per thread, three teams, a 6-deep ring of 16 KB
-    // half rows, the step's rotated words parked in TMEM during the forward transforms (53.1 ms per
-    // 2048 bootstraps; 54.1 ms with them in registers, 56.5 ms 4 deep, 62.6 ms for the plan-0 G = 2
-    // below)
+    // half rows, the step's rotated words parked in TMEM and the first two digit pairs' forward
+    // transforms interleaved (51.9 ms per 2048 bootstraps; 53.1 ms without the interleave, 54.1 ms
+    // with the words in registers, 56.5 ms 4 deep, 62.6 ms for the plan-0 G = 2 below)
+    {2048, 3, TFHEB_SPLIT_FP32, 3, 6, true, launch_paired_il<2048, 3, 3, 6, 1>, 1},
     {2048, 3, TFHEB_SPLIT_FP32, 3, 6, true, launch_paired_xt<2048, 3, 3, 6, 1>, 1},
     {2048, 3, TFHEB_SPLIT_FP32, 3, 6, true, launch_paired<2048, 3, 3, 6, 1, true>, 1},
     {2048, 3, TFHEB_SPLIT_FP32, 3, 4, true, launch_paired<2048, 3, 3, 4, 1, true>, 1},

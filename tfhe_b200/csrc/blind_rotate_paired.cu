@@ -80,7 +80,7 @@ struct PairLayout {
 // blind_rotate_kernel: the first D at the start, then each one as soon as every team has released its
 // slot, tested after each of its own half rows and waited for only when thread 0 needs one not yet
 // issued.  That frees the producer warp's registers (N = 2048 with two teams: 8 warps, 255 registers).
-template <int N, int L, int G, int D, int XB, bool PW, bool XT>
+template <int N, int L, int G, int D, int XB, bool PW, bool XT, bool IL>
 __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_paired_kernel(const BrArgs args) {
     using Lay = PairLayout<N, L, G, D, XB, PW, XT>;
     constexpr int M = N / 2, NT = M / kR, KP1 = 2, KPL = KP1 * L;
@@ -218,31 +218,21 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
             tmem_wait_st();
         }
         // 2. digits two at a time in chain order d = u*L + q, forward transforms, spectra to TMEM
-#pragma unroll
-        for (int d0 = 0; d0 < KPL; d0 += 2) {
-            const int u0 = d0 / L, q0 = d0 % L, u1 = (d0 + 1) / L, q1 = (d0 + 1) % L;
-            const int sh0 = 32 - (q0 + 1) * Bgbit, sh1 = 32 - (q1 + 1) * Bgbit;
-            uint32_t xw[KP1][2 * kR];  // XT: the words of the polynomials this pair reads, from TMEM
-            if constexpr (XT) {
-                tmem_ld16(tmem_xr + (uint32_t)(16 * u0), xw[u0]);
-                if (u1 != u0) tmem_ld16(tmem_xr + (uint32_t)(16 * u1), xw[u1]);
-                tmem_wait_ld16(xw[u0]);
-                if (u1 != u0) tmem_wait_ld16(xw[u1]);
-            }
-            const uint32_t(&xa)[2 * kR] = XT ? xw[u0] : xr[u0];
-            const uint32_t(&xb)[2 * kR] = XT ? xw[u1] : xr[u1];
-            cpair z[kR];
-            const float2 bias2 = make_float2(digit_bias, digit_bias);
+        const float2 bias2 = make_float2(digit_bias, digit_bias);
+        // digit polynomials d0 (words xa) and d0 + 1 (words xb) as one packed pair: a_j - i a_{j+M}
+        // of each (the twist is folded into the FFT)
+        auto digits = [&](cpair(&z)[kR], int d0, const uint32_t(&xa)[2 * kR], const uint32_t(&xb)[2 * kR]) {
+            const int sh0 = 32 - (d0 % L + 1) * Bgbit, sh1 = 32 - ((d0 + 1) % L + 1) * Bgbit;
 #pragma unroll
             for (int r = 0; r < kR; r++) {
-                // a_j - i a_{j+M} of each digit polynomial; the twist is folded into the FFT
                 const float2 lo = digit_pair((xa[r] >> sh0) & maskBg, (xb[r] >> sh1) & maskBg);
                 const float2 hi = digit_pair((xa[kR + r] >> sh0) & maskBg, (xb[kR + r] >> sh1) & maskBg);
                 z[r] = {sub2(lo, bias2), sub2(bias2, hi)};
             }
-            F2::forward(z, xp, s_tw2, t, bar_id);
-            // spectrum words in multiply-accumulate order: per register pair m, re(2m), re(2m+1),
-            // im(2m), im(2m+1); digit d0 then digit d0 + 1
+        };
+        // spectrum words in multiply-accumulate order: per register pair m, re(2m), re(2m+1), im(2m),
+        // im(2m+1); digit d0 then digit d0 + 1
+        auto park = [&](const cpair(&z)[kR], int d0) {
             uint32_t w[32];
 #pragma unroll
             for (int m = 0; m < kR / 2; m++) {
@@ -256,6 +246,43 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
                 w[16 + 4 * m + 3] = __float_as_uint(z[2 * m + 1].im.y);
             }
             tmem_st32(tmem_row + (uint32_t)(d0 * 16), w);
+        };
+        if constexpr (IL) {
+            // pairs (0, 1) and (2, 3) transformed together, then (4, 5)
+            static_assert(XT && L == 3 && KP1 == 2, "interleaved pairs: k = 1, l = 3, words in TMEM");
+            uint32_t xw[KP1][2 * kR];
+            tmem_ld16(tmem_xr, xw[0]);
+            tmem_ld16(tmem_xr + 16u, xw[1]);
+            tmem_wait_ld16(xw[0]);
+            tmem_wait_ld16(xw[1]);
+            cpair z0[kR], z1[kR];
+            digits(z0, 0, xw[0], xw[0]);
+            digits(z1, 2, xw[0], xw[1]);
+            F2::forward_two(z0, z1, xp, s_tw2, t, bar_id);
+            park(z0, 0);
+            park(z1, 2);
+            tmem_ld16(tmem_xr + 16u, xw[1]);
+            tmem_wait_ld16(xw[1]);
+            cpair z2[kR];
+            digits(z2, 4, xw[1], xw[1]);
+            F2::forward(z2, xp, s_tw2, t, bar_id);
+            park(z2, 4);
+        } else {
+#pragma unroll
+            for (int d0 = 0; d0 < KPL; d0 += 2) {
+                const int u0 = d0 / L, u1 = (d0 + 1) / L;
+                uint32_t xw[KP1][2 * kR];  // XT: the words of the polynomials this pair reads, from TMEM
+                if constexpr (XT) {
+                    tmem_ld16(tmem_xr + (uint32_t)(16 * u0), xw[u0]);
+                    if (u1 != u0) tmem_ld16(tmem_xr + (uint32_t)(16 * u1), xw[u1]);
+                    tmem_wait_ld16(xw[u0]);
+                    if (u1 != u0) tmem_wait_ld16(xw[u1]);
+                }
+                cpair z[kR];
+                digits(z, d0, XT ? xw[u0] : xr[u0], XT ? xw[u1] : xr[u1]);
+                F2::forward(z, xp, s_tw2, t, bar_id);
+                park(z, d0);
+            }
         }
         tmem_wait_st();
 
@@ -346,11 +373,11 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
     if (warp == 0) tmem_free(tmem_base, Lay::tmem_cols);
 }
 
-template <int N, int L, int G, int D, int XB, bool PW, bool XT>
+template <int N, int L, int G, int D, int XB, bool PW, bool XT, bool IL = false>
 static cudaError_t launch_paired_impl(const BrArgs &a, cudaStream_t s) {
     using Lay = PairLayout<N, L, G, D, XB, PW, XT>;
     if (!a.tables2) return cudaErrorInvalidValue;
-    auto kern = blind_rotate_paired_kernel<N, L, G, D, XB, PW, XT>;
+    auto kern = blind_rotate_paired_kernel<N, L, G, D, XB, PW, XT, IL>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::bytes);
     if (e != cudaSuccess) return e;
     const int grid = (a.boots + G - 1) / G;
@@ -366,6 +393,10 @@ template <int N, int L, int G, int D, int XB>
 cudaError_t launch_paired_xt(const BrArgs &a, cudaStream_t s) {
     return launch_paired_impl<N, L, G, D, XB, true, true>(a, s);
 }
+template <int N, int L, int G, int D, int XB>
+cudaError_t launch_paired_il(const BrArgs &a, cudaStream_t s) {
+    return launch_paired_impl<N, L, G, D, XB, true, true, true>(a, s);
+}
 
 template cudaError_t launch_paired<1024, 3, 7, 8, 1, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<1024, 3, 7, 12, 1, true>(const BrArgs &, cudaStream_t);
@@ -376,6 +407,8 @@ template cudaError_t launch_paired<2048, 3, 2, 4, 2, true>(const BrArgs &, cudaS
 template cudaError_t launch_paired<2048, 3, 3, 4, 1, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_xt<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_xt<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 3, 6, 1, true>(const BrArgs &, cudaStream_t);
 
 }  // namespace tfheb

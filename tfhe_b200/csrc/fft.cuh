@@ -768,6 +768,61 @@ struct TeamFft2 {
         fold_consts<false>(x);
         forward_from<0>(x, xp, tw2, t, bar_id);
     }
+
+    // Two independent forward() calls interleaved stage by stage: each stage's butterflies of x and y
+    // are independent instruction chains, each twiddle factor is loaded once for both, and the two
+    // exchanges of a stage share the buffer in turn.  Each array gets exactly forward()'s operations.
+    template <int S>
+    __device__ static __forceinline__ void twiddle_two(cpair *x, cpair *y, const float4 *tw2, int t) {
+        constexpr int r = Stage<M, S>::r, st = Stage<M, S>::stride;
+        auto apply = [&](cpair &v, cpair &u, float4 w) {
+            const float2 wr = make_float2(w.x, w.y), wi = make_float2(w.z, w.w), nwi = neg2(wi);
+            v = pmul(v, wr, wi, nwi);
+            u = pmul(u, wr, wi, nwi);
+        };
+        if constexpr (S == 0) {
+#pragma unroll
+            for (int k2 = 0; k2 < r; k2++) apply(x[k2], y[k2], tw2[k2 * NT + t]);
+        } else if constexpr (st > 1) {
+            const float4 *tws = tw2 + tw_offset<M>(S);
+#pragma unroll
+            for (int c = 0; c < R / r; c++) {
+                const int n1 = (t + NT * c) % st;
+#pragma unroll
+                for (int k2 = 1; k2 < r; k2++) apply(x[c * r + k2], y[c * r + k2], tws[(k2 - 1) * st + n1]);
+            }
+        }
+    }
+    template <int S>
+    __device__ static __forceinline__ void forward_two_from(cpair *x, cpair *y, ExchPair &xp, const float4 *tw2, int t,
+                                                            int bar_id) {
+        constexpr int r = Stage<M, S>::r;
+#pragma unroll
+        for (int c = 0; c < R / r; c++) {
+            pdft<false, r>(x + c * r);
+            pdft<false, r>(y + c * r);
+        }
+        twiddle_two<S>(x, y, tw2, t);
+        if constexpr (S + 1 < NS) {
+            void *buf = xp.next();
+            store<S, S>(x, buf, t);
+            team_sync(bar_id, NT);
+            load<S + 1, S>(x, buf, t);
+            if (xp.stride == 0) team_sync(bar_id, NT);
+            buf = xp.next();
+            store<S, S>(y, buf, t);
+            team_sync(bar_id, NT);
+            load<S + 1, S>(y, buf, t);
+            if (xp.stride == 0) team_sync(bar_id, NT);
+            forward_two_from<S + 1>(x, y, xp, tw2, t, bar_id);
+        }
+    }
+    __device__ static __forceinline__ void forward_two(cpair *x, cpair *y, ExchPair &xp, const float4 *tw2, int t,
+                                                       int bar_id) {
+        fold_consts<false>(x);
+        fold_consts<false>(y);
+        forward_two_from<0>(x, y, xp, tw2, t, bar_id);
+    }
     // TeamFft::inverse on both halves.
     __device__ static __forceinline__ void inverse(cpair *x, ExchPair &xp, const float4 *tw2, int t, int bar_id) {
         inverse_from<NS - 1>(x, xp, tw2, t, bar_id);

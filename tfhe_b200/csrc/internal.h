@@ -194,6 +194,9 @@ cudaError_t launch_paired(const BrArgs &a, cudaStream_t s);
 // the same with the step's rotated words parked in TMEM during the forward transforms
 template <int N, int L, int G, int D, int XB>
 cudaError_t launch_paired_xt(const BrArgs &a, cudaStream_t s);
+// ... and with the first two digit pairs' forward transforms interleaved stage by stage
+template <int N, int L, int G, int D, int XB>
+cudaError_t launch_paired_il(const BrArgs &a, cudaStream_t s);
 // keyswitch.cu: device key upload (both layouts) and the keyswitch of `count` extracted samples
 // (rows of in_stride int32) into rows of n+1 int32.
 cudaError_t upload_keyswitch_key(CloudKey &ck);
