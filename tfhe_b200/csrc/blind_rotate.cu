@@ -746,10 +746,14 @@ struct BrVariant {
     int plan = 0;  // 0: one transform per thread; 1: two per thread, spectra in TMEM (blind_rotate_paired.cu)
 };
 static const BrVariant kBrVariants[] = {
-    // the split default: two transforms per thread, spectra in TMEM, a 12-half-row key ring, the
-    // step's rotated words parked in TMEM and the first two digit pairs' forward transforms
-    // interleaved (31.83 ms per 4096 bootstraps, no spills; 32.24 ms for the same without the last
-    // two, 36.24 ms for the plan-0 G = 7, D = 6 below)
+    // the split default: two transforms per thread, spectra in TMEM, a 12-half-row key ring; the
+    // step's rotated words wait in TMEM, the first two digit pairs' forward transforms run
+    // interleaved, and so do both outputs' inverse transforms, output 0's input waiting in TMEM
+    // meanwhile (31.27 ms per 4096 bootstraps, no spills).  The same kernel with less interleaving:
+    // 31.59 ms (inverse input in registers, 20 B of spills), 31.85 ms (forward only), 32.2 ms (none,
+    // rotated words in registers); 36.24 ms for the plan-0 G = 7, D = 6 below.
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_il3<1024, 3, 7, 12, 1>, 1},
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_il2<1024, 3, 7, 12, 1>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_il<1024, 3, 7, 12, 1>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired<1024, 3, 7, 12, 1, true>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 6, true, launch_g<float, 1024, 3, true, 7, 6>},
@@ -760,8 +764,6 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_SPLIT_FP32, 7, 8, true, launch_paired<1024, 3, 7, 8, 1, true>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 4, true, launch_paired<1024, 3, 7, 4, 2, true>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 6, 6, true, launch_paired<1024, 3, 6, 6, 2, true>, 1},
-    // the rotated words in TMEM without the interleave: 32.4 ms
-    {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_xt<1024, 3, 7, 12, 1>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 3, 4, false, launch_g<float, 1024, 3, true, 3, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 2, 4, false, launch_g<float, 1024, 3, true, 2, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 3, true, 1, 4>},
@@ -774,13 +776,13 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_FP64, 2, 4, true, launch_g<double, 1024, 3, false, 2, 4>},
     {1024, 3, TFHEB_FP64, 1, 4, false, launch_g<double, 1024, 3, false, 1, 4>},
     {1024, 3, TFHEB_FP64, 1, 6, false, launch_wide<double, 1024, 3, false, 6, 1>},
-    // the split default at N = 2048: two transforms per thread, three teams, a 6-deep ring of 16 KB
-    // half rows, the step's rotated words parked in TMEM and the first two digit pairs' forward
-    // transforms interleaved (51.9 ms per 2048 bootstraps; 53.1 ms without the interleave, 54.1 ms
-    // with the words in registers, 56.5 ms 4 deep, 62.6 ms for the plan-0 G = 2 below)
+    // the split default at N = 2048: the N = 1024 default's structure with three teams and a 6-deep
+    // ring of 16 KB half rows (51.3 ms per 2048 bootstraps; 51.7 ms with output 0's inverse input in
+    // registers, 51.9 ms forward interleave only, 53.1 ms no interleave, 54.1 ms rotated words in
+    // registers too, 56.5 ms 4 deep, 62.6 ms for the plan-0 G = 2 below)
+    {2048, 3, TFHEB_SPLIT_FP32, 3, 6, true, launch_paired_il3<2048, 3, 3, 6, 1>, 1},
+    {2048, 3, TFHEB_SPLIT_FP32, 3, 6, true, launch_paired_il2<2048, 3, 3, 6, 1>, 1},
     {2048, 3, TFHEB_SPLIT_FP32, 3, 6, true, launch_paired_il<2048, 3, 3, 6, 1>, 1},
-    {2048, 3, TFHEB_SPLIT_FP32, 3, 6, true, launch_paired_xt<2048, 3, 3, 6, 1>, 1},
-    {2048, 3, TFHEB_SPLIT_FP32, 3, 6, true, launch_paired<2048, 3, 3, 6, 1, true>, 1},
     {2048, 3, TFHEB_SPLIT_FP32, 3, 4, true, launch_paired<2048, 3, 3, 4, 1, true>, 1},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_g<float, 2048, 3, true, 2, 4, false>},
     {2048, 3, TFHEB_SPLIT_FP32, 2, 4, true, launch_g<float, 2048, 3, true, 2, 4>},

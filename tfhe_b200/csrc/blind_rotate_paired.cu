@@ -16,9 +16,14 @@
 //   * The key ring holds half rows, one output polynomial's slots of one digit row (8 KB at N =
 //     1024), streamed in the order of the multiply-accumulate: per step, output 0 over the digits,
 //     then output 1.
-//   * XT variants also park the step's rotated words (32 per thread) in TMEM between the rotation
-//     and the digit extraction of each transform pair, so that they hold no registers across the
-//     forward transforms.
+//   * XT: the step's rotated words (32 per thread) wait in TMEM, in columns the spectra leave free,
+//     between the rotation and the digit extraction, so they hold no registers across the forward
+//     transforms.  IL (with XT): 1 transforms the first two digit pairs together, stage by stage
+//     (TeamFft2::forward_two: independent chains, one twiddle load for both); 2 also runs both
+//     outputs' multiply-accumulates first and their inverse pairs together (inverse_two); 3 as 2,
+//     with output 0's inverse input waiting in the rotated words' columns during output 1's
+//     multiply-accumulate.  Every accumulator and transform still sees the same operations in the
+//     same order, so all variants give the same bits.
 // Every mbarrier wait is bounded as in blind_rotate_kernel.  Warp 0 allocates the TMEM columns at
 // the start and frees them after every consumer thread has passed a final barrier, on every path
 // (a wait that runs out only makes the remaining waits return at once).
@@ -80,7 +85,7 @@ struct PairLayout {
 // blind_rotate_kernel: the first D at the start, then each one as soon as every team has released its
 // slot, tested after each of its own half rows and waited for only when thread 0 needs one not yet
 // issued.  That frees the producer warp's registers (N = 2048 with two teams: 8 warps, 255 registers).
-template <int N, int L, int G, int D, int XB, bool PW, bool XT, bool IL>
+template <int N, int L, int G, int D, int XB, bool PW, bool XT, int IL>
 __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_paired_kernel(const BrArgs args) {
     using Lay = PairLayout<N, L, G, D, XB, PW, XT>;
     constexpr int M = N / 2, NT = M / kR, KP1 = 2, KPL = KP1 * L;
@@ -247,7 +252,7 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
             }
             tmem_st32(tmem_row + (uint32_t)(d0 * 16), w);
         };
-        if constexpr (IL) {
+        if constexpr (IL >= 1) {
             // pairs (0, 1) and (2, 3) transformed together, then (4, 5)
             static_assert(XT && L == 3 && KP1 == 2, "interleaved pairs: k = 1, l = 3, words in TMEM");
             uint32_t xw[KP1][2 * kR];
@@ -288,9 +293,7 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
 
         // 3. per output polynomial: multiply-accumulate over the digits against the key half rows,
         //    then both limbs' inverse transforms together, exact rounding, accumulate
-#pragma unroll 1
-        for (int v = 0; v < KP1; v++) {
-            cpair ah[kR / 2], al[kR / 2];
+        auto mac = [&](int v, cpair(&ah)[kR / 2], cpair(&al)[kR / 2]) {
 #pragma unroll
             for (int m = 0; m < kR / 2; m++) {
                 ah[m] = {{0.f, 0.f}, {0.f, 0.f}};
@@ -335,20 +338,68 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
                 }
                 if (d + 1 < KPL) tmem_wait_ld16(fb[(d + 1) & 1]);
             }
-            // (hi, lo) per slot for the paired inverse
-            cpair x[kR];
+        };
+        // (hi, lo) per slot for the paired inverse
+        auto limbs = [&](cpair(&x)[kR], const cpair(&ah)[kR / 2], const cpair(&al)[kR / 2]) {
 #pragma unroll
             for (int m = 0; m < kR / 2; m++) {
                 x[2 * m] = {make_float2(ah[m].re.x, al[m].re.x), make_float2(ah[m].im.x, al[m].im.x)};
                 x[2 * m + 1] = {make_float2(ah[m].re.y, al[m].re.y), make_float2(ah[m].im.y, al[m].im.y)};
             }
-            F2::inverse(x, xp, s_tw2, t, bar_id);
+        };
+        auto accumulate = [&](int v, const cpair(&x)[kR]) {
             uint32_t *poly = s_acc + v * N;
 #pragma unroll
             for (int r = 0; r < kR; r++) {  // (c_j - i c_{j+M}) of each limb, the high limb weighted 2^S
                 const int j = t + NT * r;
                 poly[j] += (round_f32_mod32(x[r].re.x) << args.split_shift) + (uint32_t)__float2ll_rn(x[r].re.y);
                 poly[j + M] += (round_f32_mod32(-x[r].im.x) << args.split_shift) + (uint32_t)__float2ll_rn(-x[r].im.y);
+            }
+        };
+        if constexpr (IL == 3) {
+            // output 0's inverse input waits in the rotated words' TMEM columns (free after the
+            // forward transforms) during output 1's multiply-accumulate; then both inverse pairs
+            // interleaved
+            cpair x0[kR], x1[kR];
+            {
+                cpair ah[kR / 2], al[kR / 2];
+                mac(0, ah, al);
+                limbs(x0, ah, al);
+            }
+            tmem_st32(tmem_xr, reinterpret_cast<uint32_t(&)[32]>(x0));
+            {
+                cpair ah[kR / 2], al[kR / 2];
+                mac(1, ah, al);
+                limbs(x1, ah, al);
+            }
+            tmem_wait_st();
+            tmem_ld16(tmem_xr, reinterpret_cast<uint32_t(&)[16]>(x0[0]));
+            tmem_ld16(tmem_xr + 16u, reinterpret_cast<uint32_t(&)[16]>(x0[kR / 2]));
+            tmem_wait_ld16(reinterpret_cast<uint32_t(&)[16]>(x0[0]));
+            tmem_wait_ld16(reinterpret_cast<uint32_t(&)[16]>(x0[kR / 2]));
+            F2::inverse_two(x0, x1, xp, s_tw2, t, bar_id);
+            accumulate(0, x0);
+            accumulate(1, x1);
+        } else if constexpr (IL == 2) {
+            // both outputs' accumulators, then both inverse pairs interleaved
+            cpair ah0[kR / 2], al0[kR / 2], ah1[kR / 2], al1[kR / 2];
+            mac(0, ah0, al0);
+            mac(1, ah1, al1);
+            cpair x0[kR], x1[kR];
+            limbs(x0, ah0, al0);
+            limbs(x1, ah1, al1);
+            F2::inverse_two(x0, x1, xp, s_tw2, t, bar_id);
+            accumulate(0, x0);
+            accumulate(1, x1);
+        } else {
+#pragma unroll 1
+            for (int v = 0; v < KP1; v++) {
+                cpair ah[kR / 2], al[kR / 2];
+                mac(v, ah, al);
+                cpair x[kR];
+                limbs(x, ah, al);
+                F2::inverse(x, xp, s_tw2, t, bar_id);
+                accumulate(v, x);
             }
         }
         team_sync(bar_id, NT);
@@ -373,7 +424,7 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
     if (warp == 0) tmem_free(tmem_base, Lay::tmem_cols);
 }
 
-template <int N, int L, int G, int D, int XB, bool PW, bool XT, bool IL = false>
+template <int N, int L, int G, int D, int XB, bool PW, bool XT, int IL = 0>
 static cudaError_t launch_paired_impl(const BrArgs &a, cudaStream_t s) {
     using Lay = PairLayout<N, L, G, D, XB, PW, XT>;
     if (!a.tables2) return cudaErrorInvalidValue;
@@ -390,12 +441,16 @@ cudaError_t launch_paired(const BrArgs &a, cudaStream_t s) {
     return launch_paired_impl<N, L, G, D, XB, PW, false>(a, s);
 }
 template <int N, int L, int G, int D, int XB>
-cudaError_t launch_paired_xt(const BrArgs &a, cudaStream_t s) {
-    return launch_paired_impl<N, L, G, D, XB, true, true>(a, s);
+cudaError_t launch_paired_il(const BrArgs &a, cudaStream_t s) {
+    return launch_paired_impl<N, L, G, D, XB, true, true, 1>(a, s);
 }
 template <int N, int L, int G, int D, int XB>
-cudaError_t launch_paired_il(const BrArgs &a, cudaStream_t s) {
-    return launch_paired_impl<N, L, G, D, XB, true, true, true>(a, s);
+cudaError_t launch_paired_il2(const BrArgs &a, cudaStream_t s) {
+    return launch_paired_impl<N, L, G, D, XB, true, true, 2>(a, s);
+}
+template <int N, int L, int G, int D, int XB>
+cudaError_t launch_paired_il3(const BrArgs &a, cudaStream_t s) {
+    return launch_paired_impl<N, L, G, D, XB, true, true, 3>(a, s);
 }
 
 template cudaError_t launch_paired<1024, 3, 7, 8, 1, true>(const BrArgs &, cudaStream_t);
@@ -405,10 +460,11 @@ template cudaError_t launch_paired<1024, 3, 6, 6, 2, true>(const BrArgs &, cudaS
 template cudaError_t launch_paired<2048, 3, 2, 4, 2, false>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 2, 4, 2, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<2048, 3, 3, 4, 1, true>(const BrArgs &, cudaStream_t);
-template cudaError_t launch_paired_xt<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
-template cudaError_t launch_paired_xt<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
-template cudaError_t launch_paired<2048, 3, 3, 6, 1, true>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il2<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il2<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il3<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il3<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
 
 }  // namespace tfheb

@@ -828,6 +828,58 @@ struct TeamFft2 {
         inverse_from<NS - 1>(x, xp, tw2, t, bar_id);
         fold_consts<true>(x);
     }
+    // Two independent inverse() calls interleaved stage by stage (as forward_two).
+    template <int S>
+    __device__ static __forceinline__ void twiddle_conj_two(cpair *x, cpair *y, const float4 *tw2, int t) {
+        constexpr int r = Stage<M, S>::r, st = Stage<M, S>::stride;
+        auto apply = [&](cpair &v, cpair &u, float4 w) {
+            const float2 wr = make_float2(w.x, w.y), wi = make_float2(w.z, w.w), nwi = neg2(wi);
+            v = pmulconj(v, wr, wi, nwi);
+            u = pmulconj(u, wr, wi, nwi);
+        };
+        if constexpr (S == 0) {
+#pragma unroll
+            for (int k2 = 0; k2 < r; k2++) apply(x[k2], y[k2], tw2[k2 * NT + t]);
+        } else if constexpr (st > 1) {
+            const float4 *tws = tw2 + tw_offset<M>(S);
+#pragma unroll
+            for (int c = 0; c < R / r; c++) {
+                const int n1 = (t + NT * c) % st;
+#pragma unroll
+                for (int k2 = 1; k2 < r; k2++) apply(x[c * r + k2], y[c * r + k2], tws[(k2 - 1) * st + n1]);
+            }
+        }
+    }
+    template <int S>
+    __device__ static __forceinline__ void inverse_two_from(cpair *x, cpair *y, ExchPair &xp, const float4 *tw2, int t,
+                                                            int bar_id) {
+        constexpr int r = Stage<M, S>::r;
+        twiddle_conj_two<S>(x, y, tw2, t);
+#pragma unroll
+        for (int c = 0; c < R / r; c++) {
+            pdft<true, r>(x + c * r);
+            pdft<true, r>(y + c * r);
+        }
+        if constexpr (S > 0) {
+            void *buf = xp.next();
+            store<S, S - 1>(x, buf, t);
+            team_sync(bar_id, NT);
+            load<S - 1, S - 1>(x, buf, t);
+            if (xp.stride == 0) team_sync(bar_id, NT);
+            buf = xp.next();
+            store<S, S - 1>(y, buf, t);
+            team_sync(bar_id, NT);
+            load<S - 1, S - 1>(y, buf, t);
+            if (xp.stride == 0) team_sync(bar_id, NT);
+            inverse_two_from<S - 1>(x, y, xp, tw2, t, bar_id);
+        }
+    }
+    __device__ static __forceinline__ void inverse_two(cpair *x, cpair *y, ExchPair &xp, const float4 *tw2, int t,
+                                                       int bar_id) {
+        inverse_two_from<NS - 1>(x, y, xp, tw2, t, bar_id);
+        fold_consts<true>(x);
+        fold_consts<true>(y);
+    }
 };
 
 }  // namespace tfheb

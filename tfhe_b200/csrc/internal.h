@@ -191,12 +191,16 @@ cudaError_t launch_extern_product(const tfheb_params &p, int precision, const De
 struct BrArgs;
 template <int N, int L, int G, int D, int XB, bool PW>
 cudaError_t launch_paired(const BrArgs &a, cudaStream_t s);
-// the same with the step's rotated words parked in TMEM during the forward transforms
-template <int N, int L, int G, int D, int XB>
-cudaError_t launch_paired_xt(const BrArgs &a, cudaStream_t s);
-// ... and with the first two digit pairs' forward transforms interleaved stage by stage
+// the same with a producer warp, the step's rotated words parked in TMEM during the forward
+// transforms, and the first two digit pairs' forward transforms interleaved (il); also both outputs'
+// inverse transforms interleaved (il2); also output 0's inverse input parked in TMEM during output
+// 1's multiply-accumulate (il3)
 template <int N, int L, int G, int D, int XB>
 cudaError_t launch_paired_il(const BrArgs &a, cudaStream_t s);
+template <int N, int L, int G, int D, int XB>
+cudaError_t launch_paired_il2(const BrArgs &a, cudaStream_t s);
+template <int N, int L, int G, int D, int XB>
+cudaError_t launch_paired_il3(const BrArgs &a, cudaStream_t s);
 // keyswitch.cu: device key upload (both layouts) and the keyswitch of `count` extracted samples
 // (rows of in_stride int32) into rows of n+1 int32.
 cudaError_t upload_keyswitch_key(CloudKey &ck);
