@@ -767,6 +767,13 @@ static const BrVariant kBrVariants[] = {
     {1024, 3, TFHEB_SPLIT_FP32, 3, 4, false, launch_g<float, 1024, 3, true, 3, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 2, 4, false, launch_g<float, 1024, 3, true, 2, 4>},
     {1024, 3, TFHEB_SPLIT_FP32, 1, 4, false, launch_g<float, 1024, 3, true, 1, 4>},
+    // the default's kernel with 3-6 teams, for batches of one wave (later than plan 0's equals, so
+    // the default small-batch rule takes them): one wave of 148 G bootstraps in 4.78 / 5.03 / 6.12 /
+    // 6.59 ms at G = 3 / 4 / 5 / 6, against 5.64 (G = 4) and 6.85 ms (G = 5) for plan 0
+    {1024, 3, TFHEB_SPLIT_FP32, 6, 12, false, launch_paired_il3<1024, 3, 6, 12, 1>, 1},
+    {1024, 3, TFHEB_SPLIT_FP32, 5, 12, false, launch_paired_il3<1024, 3, 5, 12, 1>, 1},
+    {1024, 3, TFHEB_SPLIT_FP32, 4, 12, false, launch_paired_il3<1024, 3, 4, 12, 1>, 1},
+    {1024, 3, TFHEB_SPLIT_FP32, 3, 12, false, launch_paired_il3<1024, 3, 3, 12, 1>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 1, 8, false, launch_wide<float, 1024, 3, true, 8, 2>},
     {1024, 3, TFHEB_FP64, 4, 5, true, launch_g<double, 1024, 3, false, 4, 5, false>},
     {1024, 3, TFHEB_FP64, 4, 4, true, launch_g<double, 1024, 3, false, 4, 4, false>},

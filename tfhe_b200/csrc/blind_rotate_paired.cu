@@ -466,5 +466,9 @@ template cudaError_t launch_paired_il2<1024, 3, 7, 12, 1>(const BrArgs &, cudaSt
 template cudaError_t launch_paired_il2<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il3<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il3<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il3<1024, 3, 6, 12, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il3<1024, 3, 5, 12, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il3<1024, 3, 4, 12, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il3<1024, 3, 3, 12, 1>(const BrArgs &, cudaStream_t);
 
 }  // namespace tfheb
