@@ -749,9 +749,12 @@ static const BrVariant kBrVariants[] = {
     // the split default: two transforms per thread, spectra in TMEM, a 12-half-row key ring; the
     // step's rotated words wait in TMEM, the first two digit pairs' forward transforms run
     // interleaved, and so do both outputs' inverse transforms, output 0's input waiting in TMEM
-    // meanwhile (31.27 ms per 4096 bootstraps, no spills).  The same kernel with less interleaving:
-    // 31.59 ms (inverse input in registers, 20 B of spills), 31.85 ms (forward only), 32.2 ms (none,
-    // rotated words in registers); 36.24 ms for the plan-0 G = 7, D = 6 below.
+    // meanwhile; the keys of a digit's first two slot pairs load during the previous digit's
+    // multiply-accumulate (30.94 ms per 4096 bootstraps, no spills).  The same kernel without that
+    // prefetch: 31.27 ms; with less interleaving: 31.59 ms (inverse input in registers, 20 B of
+    // spills), 31.85 ms (forward only), 32.2 ms (none, rotated words in registers); 36.24 ms for the
+    // plan-0 G = 7, D = 6 below.
+    {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_il7<1024, 3, 7, 12, 1>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_il3<1024, 3, 7, 12, 1>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_il2<1024, 3, 7, 12, 1>, 1},
     {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_il<1024, 3, 7, 12, 1>, 1},

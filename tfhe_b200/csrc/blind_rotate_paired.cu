@@ -22,7 +22,8 @@
 //     (TeamFft2::forward_two: independent chains, one twiddle load for both); 2 also runs both
 //     outputs' multiply-accumulates first and their inverse pairs together (inverse_two); 3 as 2,
 //     with output 0's inverse input waiting in the rotated words' columns during output 1's
-//     multiply-accumulate.  Every accumulator and transform still sees the same operations in the
+//     multiply-accumulate; 7 as 3, with the keys of slot pairs 0 and 1 of digit d + 1 loaded during
+//     digit d's multiply-accumulate (16 registers of look-ahead).  Every accumulator and transform still sees the same operations in the
 //     same order, so all variants give the same bits.
 // Every mbarrier wait is bounded as in blind_rotate_kernel.  Warp 0 allocates the TMEM columns at
 // the start and frees them after every consumer thread has passed a final barrier, on every path
@@ -299,6 +300,56 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
                 ah[m] = {{0.f, 0.f}, {0.f, 0.f}};
                 al[m] = {{0.f, 0.f}, {0.f, 0.f}};
             }
+            if constexpr (IL == 7) {
+                // the keys of slot pairs 0 and 1 of digit d + 1 load during digit d's arithmetic
+                static_assert(PW, "IL = 7 needs the producer warp");
+                const int c0 = (step * KP1 + v) * KPL;
+                auto slot = [&](int c) {
+                    return reinterpret_cast<const float4 *>(smem + Lay::ring + (size_t)(c % D) * Lay::half) + t;
+                };
+                auto mac_m = [&](int m, const uint32_t(&f)[16], float4 kh, float4 kl) {
+                    const cpair zp{make_float2(__uint_as_float(f[4 * m]), __uint_as_float(f[4 * m + 1])),
+                                   make_float2(__uint_as_float(f[4 * m + 2]), __uint_as_float(f[4 * m + 3]))};
+                    const float2 nzi = mul2(zp.im, make_float2(-1.f, -1.f));
+                    cmac_pair(ah[m], zp, nzi, kh);
+                    cmac_pair(al[m], zp, nzi, kl);
+                };
+                uint32_t fb[2][16];
+                tmem_ld16(tmem_row, fb[0]);
+                wait_bounded(full_bar(c0 % D), (c0 / D) & 1, abort_flag, args.timeout_ns, args.err);
+                float4 kn[4];
+                {
+                    const float4 *kp = slot(c0);
+#pragma unroll
+                    for (int e = 0; e < 4; e++) kn[e] = kp[e * NT];
+                }
+                tmem_wait_ld16(fb[0]);
+#pragma unroll
+                for (int d = 0; d < KPL; d++) {
+                    const int c = c0 + d;
+                    const float4 *kp = slot(c);
+                    uint32_t(&f)[16] = fb[d & 1];
+                    if (d + 1 < KPL) tmem_ld16(tmem_row + (uint32_t)((d + 1) * 16), fb[(d + 1) & 1]);
+                    float4 kc[4], k2[4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) kc[e] = kn[e];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) k2[e] = kp[(4 + e) * NT];
+                    if (d + 1 < KPL) {
+                        wait_bounded(full_bar((c + 1) % D), ((c + 1) / D) & 1, abort_flag, args.timeout_ns, args.err);
+                        const float4 *kq = slot(c + 1);
+#pragma unroll
+                        for (int e = 0; e < 4; e++) kn[e] = kq[e * NT];
+                    }
+                    mac_m(0, f, kc[0], kc[1]);
+                    mac_m(1, f, kc[2], kc[3]);
+                    mac_m(2, f, k2[0], k2[1]);
+                    mac_m(3, f, k2[2], k2[3]);
+                    mbar_arrive(empty_bar(c % D));
+                    if (d + 1 < KPL) tmem_wait_ld16(fb[(d + 1) & 1]);
+                }
+                return;
+            }
             // digit spectra from TMEM, the next one loading while this one is multiplied
             uint32_t fb[2][16];
             tmem_ld16(tmem_row, fb[0]);
@@ -356,7 +407,7 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
                 poly[j + M] += (round_f32_mod32(-x[r].im.x) << args.split_shift) + (uint32_t)__float2ll_rn(-x[r].im.y);
             }
         };
-        if constexpr (IL == 3) {
+        if constexpr (IL == 3 || IL == 7) {
             // output 0's inverse input waits in the rotated words' TMEM columns (free after the
             // forward transforms) during output 1's multiply-accumulate; then both inverse pairs
             // interleaved
@@ -452,6 +503,10 @@ template <int N, int L, int G, int D, int XB>
 cudaError_t launch_paired_il3(const BrArgs &a, cudaStream_t s) {
     return launch_paired_impl<N, L, G, D, XB, true, true, 3>(a, s);
 }
+template <int N, int L, int G, int D, int XB>
+cudaError_t launch_paired_il7(const BrArgs &a, cudaStream_t s) {
+    return launch_paired_impl<N, L, G, D, XB, true, true, 7>(a, s);
+}
 
 template cudaError_t launch_paired<1024, 3, 7, 8, 1, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<1024, 3, 7, 12, 1, true>(const BrArgs &, cudaStream_t);
@@ -466,6 +521,8 @@ template cudaError_t launch_paired_il2<1024, 3, 7, 12, 1>(const BrArgs &, cudaSt
 template cudaError_t launch_paired_il2<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il3<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il3<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
+template cudaError_t launch_paired_il7<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
+
 template cudaError_t launch_paired_il3<1024, 3, 6, 12, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il3<1024, 3, 5, 12, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il3<1024, 3, 4, 12, 1>(const BrArgs &, cudaStream_t);

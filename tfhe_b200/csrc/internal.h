@@ -194,13 +194,15 @@ cudaError_t launch_paired(const BrArgs &a, cudaStream_t s);
 // the same with a producer warp, the step's rotated words parked in TMEM during the forward
 // transforms, and the first two digit pairs' forward transforms interleaved (il); also both outputs'
 // inverse transforms interleaved (il2); also output 0's inverse input parked in TMEM during output
-// 1's multiply-accumulate (il3)
+// 1's multiply-accumulate (il3); also half of each digit's keys loaded one digit ahead (il7)
 template <int N, int L, int G, int D, int XB>
 cudaError_t launch_paired_il(const BrArgs &a, cudaStream_t s);
 template <int N, int L, int G, int D, int XB>
 cudaError_t launch_paired_il2(const BrArgs &a, cudaStream_t s);
 template <int N, int L, int G, int D, int XB>
 cudaError_t launch_paired_il3(const BrArgs &a, cudaStream_t s);
+template <int N, int L, int G, int D, int XB>
+cudaError_t launch_paired_il7(const BrArgs &a, cudaStream_t s);
 // keyswitch.cu: device key upload (both layouts) and the keyswitch of `count` extracted samples
 // (rows of in_stride int32) into rows of n+1 int32.
 cudaError_t upload_keyswitch_key(CloudKey &ck);
