@@ -750,8 +750,9 @@ static const BrVariant kBrVariants[] = {
     // step's rotated words wait in TMEM, the first two digit pairs' forward transforms run
     // interleaved, and so do both outputs' inverse transforms, output 0's input waiting in TMEM
     // meanwhile; the keys of a digit's first two slot pairs load during the previous digit's
-    // multiply-accumulate (30.94 ms per 4096 bootstraps, no spills).  The same kernel without that
-    // prefetch: 31.27 ms; with less interleaving: 31.59 ms (inverse input in registers, 20 B of
+    // multiply-accumulate (30.94 ms per 4096 bootstraps, no spills; on another box 31.50 against
+    // 31.33 ms without it, so both stay candidates and the autotuner picks).  The same kernel
+    // without that prefetch: 31.27 ms; loading 3 or 4 slot pairs ahead: 31.49 / 31.68 ms; with less interleaving: 31.59 ms (inverse input in registers, 20 B of
     // spills), 31.85 ms (forward only), 32.2 ms (none, rotated words in registers); 36.24 ms for the
     // plan-0 G = 7, D = 6 below.
     {1024, 3, TFHEB_SPLIT_FP32, 7, 12, true, launch_paired_il7<1024, 3, 7, 12, 1>, 1},

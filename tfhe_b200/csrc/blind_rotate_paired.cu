@@ -301,8 +301,9 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
                 al[m] = {{0.f, 0.f}, {0.f, 0.f}};
             }
             if constexpr (IL == 7) {
-                // the keys of slot pairs 0 and 1 of digit d + 1 load during digit d's arithmetic
+                // the keys of the first PF slot pairs of digit d + 1 load during digit d's arithmetic
                 static_assert(PW, "IL = 7 needs the producer warp");
+                constexpr int PF = 2;  // slot pairs (2 float4 each) ahead; 3 or 4 measured no faster
                 const int c0 = (step * KP1 + v) * KPL;
                 auto slot = [&](int c) {
                     return reinterpret_cast<const float4 *>(smem + Lay::ring + (size_t)(c % D) * Lay::half) + t;
@@ -317,11 +318,11 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
                 uint32_t fb[2][16];
                 tmem_ld16(tmem_row, fb[0]);
                 wait_bounded(full_bar(c0 % D), (c0 / D) & 1, abort_flag, args.timeout_ns, args.err);
-                float4 kn[4];
+                float4 kn[2 * PF];
                 {
                     const float4 *kp = slot(c0);
 #pragma unroll
-                    for (int e = 0; e < 4; e++) kn[e] = kp[e * NT];
+                    for (int e = 0; e < 2 * PF; e++) kn[e] = kp[e * NT];
                 }
                 tmem_wait_ld16(fb[0]);
 #pragma unroll
@@ -330,21 +331,19 @@ __global__ void __launch_bounds__(G *(N / 16) + (PW ? 32 : 0), 1) blind_rotate_p
                     const float4 *kp = slot(c);
                     uint32_t(&f)[16] = fb[d & 1];
                     if (d + 1 < KPL) tmem_ld16(tmem_row + (uint32_t)((d + 1) * 16), fb[(d + 1) & 1]);
-                    float4 kc[4], k2[4];
+                    float4 kc[kR];  // this digit's keys: the first 2 PF from the look-ahead
 #pragma unroll
-                    for (int e = 0; e < 4; e++) kc[e] = kn[e];
+                    for (int e = 0; e < 2 * PF; e++) kc[e] = kn[e];
 #pragma unroll
-                    for (int e = 0; e < 4; e++) k2[e] = kp[(4 + e) * NT];
+                    for (int e = 2 * PF; e < kR; e++) kc[e] = kp[e * NT];
                     if (d + 1 < KPL) {
                         wait_bounded(full_bar((c + 1) % D), ((c + 1) / D) & 1, abort_flag, args.timeout_ns, args.err);
                         const float4 *kq = slot(c + 1);
 #pragma unroll
-                        for (int e = 0; e < 4; e++) kn[e] = kq[e * NT];
+                        for (int e = 0; e < 2 * PF; e++) kn[e] = kq[e * NT];
                     }
-                    mac_m(0, f, kc[0], kc[1]);
-                    mac_m(1, f, kc[2], kc[3]);
-                    mac_m(2, f, k2[0], k2[1]);
-                    mac_m(3, f, k2[2], k2[3]);
+#pragma unroll
+                    for (int m = 0; m < kR / 2; m++) mac_m(m, f, kc[2 * m], kc[2 * m + 1]);
                     mbar_arrive(empty_bar(c % D));
                     if (d + 1 < KPL) tmem_wait_ld16(fb[(d + 1) & 1]);
                 }
@@ -508,6 +507,7 @@ cudaError_t launch_paired_il7(const BrArgs &a, cudaStream_t s) {
     return launch_paired_impl<N, L, G, D, XB, true, true, 7>(a, s);
 }
 
+
 template cudaError_t launch_paired<1024, 3, 7, 8, 1, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<1024, 3, 7, 12, 1, true>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired<1024, 3, 7, 4, 2, true>(const BrArgs &, cudaStream_t);
@@ -522,6 +522,7 @@ template cudaError_t launch_paired_il2<2048, 3, 3, 6, 1>(const BrArgs &, cudaStr
 template cudaError_t launch_paired_il3<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il3<2048, 3, 3, 6, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il7<1024, 3, 7, 12, 1>(const BrArgs &, cudaStream_t);
+
 
 template cudaError_t launch_paired_il3<1024, 3, 6, 12, 1>(const BrArgs &, cudaStream_t);
 template cudaError_t launch_paired_il3<1024, 3, 5, 12, 1>(const BrArgs &, cudaStream_t);
