@@ -577,7 +577,8 @@ def main():
             "peaks_measured": peak,
             "autotune": tuning,
             "plans": {"0": "radix-8 team FFT, one transform per thread",
-                      "1": "radix-8 team FFT, two transforms per thread on packed f32x2, digit spectra in TMEM"},
+                      "1": "radix-8 team FFT, two transforms per thread on packed f32x2, digit spectra in TMEM "
+                           "(candidates differ in ring depth and in how many transform pairs run interleaved)"},
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * B * (p.n + 1) * 4,
                     "d2h_bytes_per_step": B * (p.n + 1) * 4, "errors": e2e_errors,
