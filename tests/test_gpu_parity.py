@@ -154,6 +154,36 @@ def test_keyswitch_tiled_large_params_bit_exact(oracle, large_keys):
     assert (tiled[[0, 129]] == oracle.keyswitch(pdict(p), ksk, x[[0, 129]])).all()
 
 
+# the tensor-core kernel's tile edges (256 samples per CTA: 255 / 256 / 257; those split the
+# coefficient range over CTAs and combine with atomic adds) and 7421 samples, 29 tiles x 10 column
+# groups = 290 CTAs, which its wave model runs with one coefficient range per CTA (plain stores);
+# every kernel must agree bit for bit
+@pytest.mark.parametrize("count", [255, 256, 257, 7421])
+def test_keyswitch_tensor_core_tile_edges(oracle, default_keys, count):
+    p, sk, ck, bsk, ksk = default_keys
+    rng = np.random.default_rng(300 + count)
+    x = rng.integers(-2**31, 2**31, (count, p.k * p.N + 1), dtype=np.int64).astype(np.int32)
+    x[-1] = 0
+    tensor_core = _keyswitch_with(ck, p, x, 4, 11)
+    assert (tensor_core == _keyswitch_with(ck, p, x, 3, -11)).all()
+    assert (tensor_core == _keyswitch_with(ck, p, x, 0, 5)).all()  # the default is the tensor-core kernel
+    pick = sorted({0, 255 % count, count - 1})
+    assert (tensor_core[pick] == oracle.keyswitch(pdict(p), ksk, x[pick])).all()
+
+
+def test_keyswitch_tensor_core_80bit_partial_column_group(oracle):
+    # n = 500: 501 output columns, the last 64-column group holds 53 of them
+    p = tb.default_params(80)
+    sk, ck = tb.keygen(p, seed=80)
+    ck.to_device(0, precisions=(tb.FP64,))
+    bsk, ksk = ck.export()
+    rng = np.random.default_rng(81)
+    x = rng.integers(-2**31, 2**31, (300, p.k * p.N + 1), dtype=np.int64).astype(np.int32)
+    tensor_core = _keyswitch_with(ck, p, x, 4, 9)
+    assert (tensor_core == _keyswitch_with(ck, p, x, 1, 0)).all()
+    assert (tensor_core[[0, 299]] == oracle.keyswitch(pdict(p), ksk, x[[0, 299]])).all()
+
+
 # ---------------------------------------------------------------------------------------------
 # one CMUX step = rotation + decomposition + external product: exact (FP64) / bounded (split)
 # ---------------------------------------------------------------------------------------------
