@@ -106,7 +106,9 @@ def test_calls_on_two_streams_use_the_key_scratch_in_order(keys):
 @pytest.mark.parametrize("precision", [tb.FP64, tb.SPLIT_FP32])
 def test_small_batches_match_large_batches_bit_for_bit(keys, precision):
     # 20 gates fit one wave with one bootstrap per CTA, so they run on a small-batch variant (or, after
-    # the autotuner, on whatever it measured fastest); 2000 gates run on the tuned variant
+    # the autotuner, on whatever it measured fastest); 300 / 592 / 740 / 888 gates need 3 / 4 / 5 / 6
+    # bootstraps per CTA (148 SMs), the small-batch variants with that many teams; 2000 gates run on
+    # the tuned variant
     p, sk, ck = keys
     rng = np.random.default_rng(90 + precision)
     x, y = rng.integers(0, 2, 2000), rng.integers(0, 2, 2000)
@@ -115,9 +117,9 @@ def test_small_batches_match_large_batches_bit_for_bit(keys, precision):
         if tuned:
             ck.autotune(precision, boots=2000)
         big = ck.gate(tb.api.NAND, a, b, precision=precision)
-        small = ck.gate(tb.api.NAND, a[:20], b[:20], precision=precision)
-        mid = ck.gate(tb.api.NAND, a[:300], b[:300], precision=precision)
-        assert (small == big[:20]).all() and (mid == big[:300]).all()
+        for n_ in (20, 300, 592, 740, 888):
+            part = ck.gate(tb.api.NAND, a[:n_], b[:n_], precision=precision)
+            assert (part == big[:n_]).all(), f"{n_} gates differ from the large batch"
         got, _ = sk.decrypt(big)
         assert (got == 1 - (x & y)).all()
 
