@@ -23,8 +23,8 @@
 //     outputs' multiply-accumulates first and their inverse pairs together (inverse_two); 3 as 2,
 //     with output 0's inverse input waiting in the rotated words' columns during output 1's
 //     multiply-accumulate; 7 as 3, with the keys of slot pairs 0 and 1 of digit d + 1 loaded during
-//     digit d's multiply-accumulate (16 registers of look-ahead).  Every accumulator and transform still sees the same operations in the
-//     same order, so all variants give the same bits.
+//     digit d's multiply-accumulate (16 registers of look-ahead).  Every accumulator and transform
+//     still sees the same operations in the same order, so all variants give the same bits.
 // Every mbarrier wait is bounded as in blind_rotate_kernel.  Warp 0 allocates the TMEM columns at
 // the start and frees them after every consumer thread has passed a final barrier, on every path
 // (a wait that runs out only makes the remaining waits return at once).
